@@ -1,0 +1,387 @@
+#!/usr/bin/env python
+"""ESP throughput benchmark: the 54-atom l<=3 synthetic system at 30000 vdW points.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp64|mixed] [--points 30000]
+
+A step is one evaluation of the ESP at all points of the workload with the
+pair table resident in HBM (``value``, points/s).  ``e2e`` is the same metric
+through the public API from pinned host buffers: density and points copied to
+the device, the table built, the ESP evaluated and copied back, every step.
+The table-build time is reported separately.  Under torchrun every rank
+evaluates its own 30000-point set of the same molecule (weak scaling, no
+collective on the data path); times are the max over ranks.
+
+``--impl reference`` times the reference's own CPU path on the host cores:
+its OpenMP C++ table builder (oracle/_ref/build_pairs, compiled from the
+reference's source) plus its NumPy evaluator (restated in oracle/) on a
+bounded per-class sample of pairs, scaled by the class pair counts.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = ("frag54: 54 atoms (30 C / 8 N / 8 O / 8 H), l<=3 TZ-like basis with diffuse "
+            "functions (1658 Cartesian functions, 2088 primitives), 30000 points on the "
+            "1.4x Bondi vdW surface, screening tol 1e-12")
+METRIC = "ESP points/s, 54-atom l<=3 basis: mixed vs FP64 GPU path at <=1e-6 a.u. max err"
+PUBLISHED = {"e2e_points_per_s": 30000 / 2.4564, "hardware": "RTX 5090",
+             "source": "reference README.md:48 (table build + GPU solve, 30000 points)"}
+
+
+def rank_info():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 6:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[2:6]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def peak_flops(torch, fp64=True):
+    from fastesp_b200 import _lib
+    dev = torch.cuda.current_device()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    blocks = sms * 8
+    out = torch.empty(blocks, dtype=torch.float64, device="cuda")
+    iters = 1 << 14 if fp64 else 1 << 15
+    for _ in range(2):
+        _lib.check(_lib.lib().fe_peak_run(int(fp64), iters, blocks, _lib.ptr(out), _lib.stream_ptr()))
+    best = 0.0
+    for _ in range(5):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        _lib.check(_lib.lib().fe_peak_run(int(fp64), iters, blocks, _lib.ptr(out), _lib.stream_ptr()))
+        b.record()
+        b.synchronize()
+        best = max(best, 16.0 * iters * 256 * blocks / (a.elapsed_time(b) * 1e-3))
+    return best
+
+
+def algorithmic_flops(counts, npts):
+    from fastesp_b200 import hermite as H
+    return float(sum(c * H.eval_flops(L) for L, c in enumerate(counts))) * npts
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from fastesp_b200 import _lib, build_table, synth
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    wfn, basis, P, _ = synth.load_workload("frag54", 10, seed=1)
+    pts = synth.vdw_surface_points(wfn.symbols, wfn.coords, args.points, seed=1 + rank)
+    dev = torch.device("cuda", local)
+    P_d = torch.as_tensor(P, device=dev)
+    pts_d = torch.as_tensor(pts, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # table build (device-resident inputs)
+    tab = build_table(wfn, basis, P_d, pts_d, tol=1e-12)
+    counts = tab.counts
+    prec = args.precision
+    tb = []
+    for i in range(args.warmup + max(3, args.steps // 2)):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        t2 = build_table(wfn, basis, P_d, pts_d, tol=1e-12)
+        b.record()
+        b.synchronize()
+        if i >= args.warmup:
+            tb.append(a.elapsed_time(b))
+        del t2
+    build_ms = statistics.median(tb)
+
+    # value: evaluation with the table resident
+    out = torch.empty(args.points, dtype=torch.float64, device=dev)
+    L = _lib.lib()
+    ws = torch.empty(max(256, L.fe_eval_ws_bytes(args.points, 0)), dtype=torch.uint8, device=dev)
+
+    def step():
+        _lib.check(L.fe_esp_fp64(_lib.ptr(tab._buf), _lib.ptr(pts_d), args.points, _lib.ptr(out),
+                                 _lib.ptr(ws), ws.numel(), _lib.stream_ptr()))
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        step()
+    barrier()
+    times = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()            # L2 flush between timed steps (not timed)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            step()
+            b.record()
+            b.synchronize()
+            times.append(a.elapsed_time(b))
+        barrier()
+    t_ms = sum(times)
+    t_ms_max = t_ms
+    if world > 1:
+        t = torch.tensor([t_ms, build_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms_max, build_ms = float(t[0]), float(t[1])
+    ms_per_step = t_ms_max / args.steps
+    value = world * args.points / (ms_per_step * 1e-3)
+
+    # e2e through the public API from pinned host buffers
+    P_h = torch.as_tensor(P).pin_memory()
+    pts_h = torch.as_tensor(pts).pin_memory()
+    res_h = torch.empty(args.points, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        t = build_table(wfn, basis, P_h, pts_h, tol=1e-12)
+        v = t.esp(pts_h.to(dev, non_blocking=True))
+        res_h.copy_(v, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    barrier()
+    e2e_t = []
+    for _ in range(max(3, args.steps // 2)):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        e2e_step()
+        b.record()
+        b.synchronize()
+        e2e_t.append(a.elapsed_time(b))
+    e2e_ms = statistics.mean(e2e_t)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t[0])
+    e2e = {"value": world * args.points / (e2e_ms * 1e-3), "unit": "points/s",
+           "h2d_bytes_per_step": int(P_h.numel() * 8 + 2 * pts_h.numel() * 8),
+           "d2h_bytes_per_step": int(res_h.numel() * 8), "ms_per_step": e2e_ms,
+           "includes": "H2D density+points, GPU table build, GPU evaluation, D2H result"}
+
+    # parity check of this very run against the golden 300-point values
+    from fastesp_b200 import build_table as bt
+    g = np.load(ROOT / "tests" / "golden" / "frag54_300.npz")
+    gt = bt(wfn, basis, P_d, g["points"], tol=1e-12)
+    parity = float(np.abs(gt.esp() - g["esp_t12"]).max())
+    status = _lib.status(clear=True)
+
+    peak = peak_flops(torch, fp64=(prec == "fp64"))
+    flops = algorithmic_flops(counts, args.points)
+    achieved = flops / (ms_per_step * 1e-3)
+    traffic = None
+    prof = ROOT / "profiles" / "eval_f64_frag54_30000.json"
+    if prof.exists():
+        traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
+    nsplit_launches = 2 if L.fe_eval_ws_bytes(args.points, 0) > 256 else 1
+    line = {
+        "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if prec == "fp64" else "f32+f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "points_per_gpu": args.points,
+                   "pairs": int(sum(counts)), "pairs_per_class": counts,
+                   "precision": prec, "l2": "flushed (256 MiB write) between timed steps",
+                   "parallelism": f"points sharded across {world} GPU(s), table per GPU"},
+        "table_build_ms": build_ms,
+        "e2e": e2e,
+        "roofline": {"bound": "fp64" if prec == "fp64" else "fp32", "achieved": achieved / 1e12,
+                     "peak": peak / 1e12, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": traffic,
+                     "peak_source": "measured FMA throughput (fe_peak_run) on this GPU, this run",
+                     "flops_per_step": flops},
+        "gpu_launches": args.steps * nsplit_launches,
+        "parity_frag54_300_max_abs": parity,
+        "device_status": status,
+        "published_reference": PUBLISHED,
+    }
+    line["clocks"] = clk.summary()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(wfn, basis, P, pts, counts, budget_s=args.cpu_budget)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# reference CPU path (build_pairs + NumPy evaluator on a bounded sample)
+# ---------------------------------------------------------------------------
+def cpu_baseline(wfn, basis, P, pts, counts=None, budget_s=20.0, per_class=None):
+    import oracle.esp_oracle as O
+    from fastesp_b200 import basis_payload, hermite as H, write_basis_payload
+    ncore = len(os.sched_getaffinity(0))
+    exe = ROOT / "oracle" / "_ref" / "build_pairs"
+    env = dict(os.environ, OMP_NUM_THREADS=str(ncore))
+    with tempfile.TemporaryDirectory() as td:
+        bb, pb = Path(td) / "basis.bin", Path(td) / "pairs.bin"
+        write_basis_payload(bb, basis_payload(wfn, basis, P, pts))
+        if exe.exists():
+            t0 = time.perf_counter()
+            subprocess.run([str(exe), str(bb), str(pb), "1e-12"], check=True, env=env,
+                           capture_output=True)
+            t_build = time.perf_counter() - t0
+            tab = O.OracleTable.read(pb)
+            kind = "reference"
+        else:
+            t0 = time.perf_counter()
+            from fastesp_b200.molden import Z_OF
+            Z = np.array([Z_OF[s] for s in wfn.symbols])
+            tab = O.build_table(wfn.shells, wfn.coords, Z, P, pts, tol=1e-12, rule="native")
+            t_build = time.perf_counter() - t0
+            kind = "port"
+    # NumPy evaluator (fastesp/table.py:73-93) on a per-class sample, scaled
+    nt = tab.pp_nt
+    by_nt = {H.n_terms(L): L for L in range(9)}
+    cls = np.array([by_nt[int(t)] for t in nt])
+    rng = np.random.default_rng(0)
+    t_eval = 0.0
+    sampled = 0
+    per_class = per_class or max(2, int(budget_s * 4))
+    for L in range(9):
+        idx = np.nonzero(cls == L)[0]
+        if not len(idx):
+            continue
+        take = rng.choice(idx, size=min(len(idx), per_class), replace=False)
+        mask = np.zeros(tab.n_pairs, bool)
+        mask[take] = True
+        t0 = time.perf_counter()
+        tab.electron(pts, pair_mask=mask)
+        dt = time.perf_counter() - t0
+        t_eval += dt * len(idx) / len(take)
+        sampled += len(take)
+    t_tot = t_build + t_eval
+    return {"value": len(pts) / t_tot, "unit": "points/s", "cores": ncore, "kind": kind,
+            "sample": (f"{'reference build_pairs (C++/OpenMP, ' + str(ncore) + ' threads)' if kind == 'reference' else 'oracle build (NumPy)'}"
+                       f" on all {len(pts)} points: {t_build:.2f} s; NumPy evaluator (1 thread) "
+                       f"timed on {sampled} sampled pairs (<= {per_class} per class) at all "
+                       f"points and scaled by class pair counts: {t_eval:.1f} s estimated"),
+            "build_s": t_build, "eval_s_estimated": t_eval, "n_pairs": int(tab.n_pairs)}
+
+
+def run_reference(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    from fastesp_b200 import synth
+    wfn, basis, P, _ = synth.load_workload("frag54", 10, seed=1)
+    pts = synth.vdw_surface_points(wfn.symbols, wfn.coords, args.points, seed=1)
+    per_step = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(wfn, basis, P, pts, budget_s=2.0, per_class=6)
+        if i >= args.warmup:
+            per_step.append(len(pts) / cb["value"])
+            base = cb
+    ms = 1e3 * statistics.mean(per_step)
+    value = len(pts) / (ms * 1e-3)
+    base = dict(base, value=value)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "points/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "points_per_gpu": args.points,
+                                             "precision": "fp64"},
+            "cpu_baseline": base,
+            "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--points", type=int, default=30000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

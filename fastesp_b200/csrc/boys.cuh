@@ -1,0 +1,58 @@
+// Boys function F_m(T) = int_0^1 t^(2m) exp(-T t^2) dt, orders 0..M at once.
+//
+// Three regimes (the method of Helgaker, Jorgensen & Olsen, Molecular
+// Electronic-Structure Theory, sec. 9.8.2: tabulated Taylor expansion plus
+// asymptotic form, with the standard recursions between orders):
+//
+//   T >= fe_boys_asym_T[M] : F_0 = sqrt(pi/T)/2 and F_(m+1) = (2m+1)/(2T) F_m.
+//                            The neglected terms are below 1e-16 relative for
+//                            all orders <= M (thresholds computed in 40-digit
+//                            arithmetic by gen_classes.py).
+//   12 <= T < threshold    : F_0 = sqrt(pi/T)/2 erf(sqrt T) and the upward
+//                            recursion F_(m+1) = ((2m+1) F_m - e^-T)/(2T), which
+//                            loses at most a few percent of an ulp per step at
+//                            T >= 12 for m <= 9.
+//   T < 12                 : F_M from an 8-term Taylor expansion about the
+//                            nearest point of a 1/16 grid (truncation below
+//                            3e-17 relative), then the stable downward recursion
+//                            F_(m-1) = (2T F_m + e^-T)/(2m-1).
+//
+// exp, erf and rsqrt are CUDA's own; the grid values F_n(i/16) are 40-digit
+// reference values generated into classes_gen.cuh.
+#pragma once
+#include "common.cuh"
+#include "classes_gen.cuh"
+
+#define FE_SQRT_PI_2 0.88622692545275801365   // sqrt(pi)/2
+
+template <int M>
+FE_DEV void fe_boys_f64(const double T, double (&F)[M + 1]) {
+  constexpr double t_asym = fe_boys_asym_T[M];
+  if (T >= t_asym) {
+    const double r = rsqrt(T);
+    const double h = 0.5 * r * r;               // 1/(2T)
+    F[0] = FE_SQRT_PI_2 * r;
+#pragma unroll
+    for (int m = 0; m < M; ++m) F[m + 1] = F[m] * (double(2 * m + 1) * h);
+  } else if (T >= FE_BOYS_GRID_TMAX) {
+    const double r = rsqrt(T);
+    const double h = 0.5 * r * r;
+    const double e = exp(-T);
+    F[0] = FE_SQRT_PI_2 * r * erf(T * r);
+#pragma unroll
+    for (int m = 0; m < M; ++m) F[m + 1] = fma(double(2 * m + 1), F[m], -e) * h;
+  } else {
+    const int i = __double2int_rn(T * FE_BOYS_GRID_INV_H);
+    const double d = -(T - double(i) * FE_BOYS_GRID_H);   // exact: |d| <= h/2
+    const double* row = fe_boys_grid + i * FE_BOYS_NTAB + M;
+    double f = __ldg(row + FE_BOYS_TAYLOR_K - 1);
+#pragma unroll
+    for (int k = FE_BOYS_TAYLOR_K - 2; k >= 0; --k)
+      f = fma(f, d * (1.0 / double(k + 1)), __ldg(row + k));
+    F[M] = f;
+    const double e = exp(-T);
+    const double t2 = T + T;
+#pragma unroll
+    for (int m = M; m > 0; --m) F[m - 1] = fma(t2, F[m], e) * (1.0 / double(2 * m - 1));
+  }
+}

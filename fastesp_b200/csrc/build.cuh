@@ -1,0 +1,432 @@
+// Pair-table build: replaces build_pairs (fastesp/native/build_pairs.cpp:162-425)
+// and build_table / ESPEngine (fastesp/table.py:176-259, fastesp/esp.py:168-257).
+//
+// One thread per primitive pair.  Work items are grouped by the shell pair's
+// (la, lb) so that a block runs one template instance; each thread writes its
+// pair to a fixed slot of its class's staging array (slots are numbered in
+// the reference's pair order), with a keep flag.  A scan of the flags and a
+// scatter kernel then compact every class in order into the table.
+//
+// Per primitive pair (a = exponent of shell si, b = of sj):
+//   p = a + b, P = (aA + bB)/p, K = exp(-ab/p |A-B|^2)       (esp.py:226-230)
+//   E^x_t, E^y_t, E^z_t Hermite coefficients                 (esp.py:108-147)
+//   etab[t] = sum_mu,nu w_mu,nu Ex Ey Ez, w = (D_ij + D_ji) c_a c_b  (esp.py:239-247)
+//   G_k = (2 pi/p)(2p)^m_k sum_t M0[k,t] etab[t]              (esp.py:248-250)
+//   bound = (2p)^-1.5 sum_t |etab_t| M_tx M_ty M_tz (2p)^(|t|/2), reff = 1.6 sqrt((L+2)/p)
+//   screen: rule 0 keeps unless K bound / max(dmin, 0.05) < tol   (table.py:190-194)
+//           rule 1 drops if K bound / max(dmin - reff, 0.05) < tol,
+//                  and drops pairs with c_a c_b == 0 or all G == 0 (build_pairs.cpp:243,309,326-328)
+#pragma once
+#include "common.cuh"
+#include "classes_gen.cuh"
+#include "table.cuh"
+
+struct FeShell {
+  int atom, l, fn0, prim0, nprim, pad_;
+  double c[3];
+};
+
+struct FeTask {          // one shell pair (si <= sj) with a non-empty class slot range
+  int si, sj;
+  int slot0;             // class slot of primitive pair (0, 0)
+  int pad_;
+};
+
+struct FeBuildArgs {
+  const FeShell* shells;
+  const double* sexp;            // per-shell primitive exponents (shell.prim0 + i)
+  const double* scoef;           // per-shell contraction coefficients
+  const FeTask* tasks;
+  const int* work_task;          // work item -> task
+  const int* work_ij;            // work item -> (i << 16) | j
+  const int* grp_block0;         // first block of each (la, lb) group
+  const int* grp_code;           // la * 5 + lb
+  const int* grp_work0;          // first work item of each group
+  const int* grp_nwork;
+  int ngroup;
+  int n_func;
+  const double* dens;            // (n_func, n_func) Cartesian density
+  const double* pts;             // (npts, 3)
+  int npts;
+  double tol;
+  int rule;
+  const long long* class_slot0;  // first global slot of class L in the staging arrays
+  double* stage;                 // staging records, class L at stage_off[L] doubles
+  const long long* stage_off;
+  int* keep;                     // per global slot
+  double* srule;                 // per global slot: K (pi/p)^1.5 etab[0]
+};
+
+__constant__ signed char fe_cart[5][15][3] = {
+  {{0, 0, 0}},
+  {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}},
+  {{2, 0, 0}, {1, 1, 0}, {1, 0, 1}, {0, 2, 0}, {0, 1, 1}, {0, 0, 2}},
+  {{3, 0, 0}, {2, 1, 0}, {2, 0, 1}, {1, 2, 0}, {1, 1, 1}, {1, 0, 2}, {0, 3, 0}, {0, 2, 1},
+   {0, 1, 2}, {0, 0, 3}},
+  {{4, 0, 0}, {3, 1, 0}, {3, 0, 1}, {2, 2, 0}, {2, 1, 1}, {2, 0, 2}, {1, 3, 0}, {1, 2, 1},
+   {1, 1, 2}, {1, 0, 3}, {0, 4, 0}, {0, 3, 1}, {0, 2, 2}, {0, 1, 3}, {0, 0, 4}}};
+
+__constant__ double fe_screen_mom[12] = {
+  2.5066282746310002, 2.0, 1.5957691216057308, 4.0, 10.212920779565312, 33.63284766793385,
+  136.5963625280984, 665.1416330443616, 3768.863619586618, 25506.330595911374,
+  202331.81842358326, 1872154.2572862155};
+
+template <int L>
+FE_DEV int fe_tri(int tx, int ty, int tz) {
+  // compact index of (tx, ty, tz), |t| <= L, x-major then y then z
+  int base = 0;
+  for (int a = 0; a < tx; ++a) base += (L + 1 - a) * (L + 2 - a) / 2;
+  for (int b = 0; b < ty; ++b) base += L + 1 - tx - b;
+  return base + tz;
+}
+
+template <int L>
+FE_DEV const short* fe_m0_ptr() {
+  if constexpr (L == 0) return fe_m0_ptr_L0; else if constexpr (L == 1) return fe_m0_ptr_L1;
+  else if constexpr (L == 2) return fe_m0_ptr_L2; else if constexpr (L == 3) return fe_m0_ptr_L3;
+  else if constexpr (L == 4) return fe_m0_ptr_L4; else if constexpr (L == 5) return fe_m0_ptr_L5;
+  else if constexpr (L == 6) return fe_m0_ptr_L6; else if constexpr (L == 7) return fe_m0_ptr_L7;
+  else return fe_m0_ptr_L8;
+}
+template <int L>
+FE_DEV const short* fe_m0_col() {
+  if constexpr (L == 0) return fe_m0_col_L0; else if constexpr (L == 1) return fe_m0_col_L1;
+  else if constexpr (L == 2) return fe_m0_col_L2; else if constexpr (L == 3) return fe_m0_col_L3;
+  else if constexpr (L == 4) return fe_m0_col_L4; else if constexpr (L == 5) return fe_m0_col_L5;
+  else if constexpr (L == 6) return fe_m0_col_L6; else if constexpr (L == 7) return fe_m0_col_L7;
+  else return fe_m0_col_L8;
+}
+template <int L>
+FE_DEV const float* fe_m0_val() {
+  if constexpr (L == 0) return fe_m0_val_L0; else if constexpr (L == 1) return fe_m0_val_L1;
+  else if constexpr (L == 2) return fe_m0_val_L2; else if constexpr (L == 3) return fe_m0_val_L3;
+  else if constexpr (L == 4) return fe_m0_val_L4; else if constexpr (L == 5) return fe_m0_val_L5;
+  else if constexpr (L == 6) return fe_m0_val_L6; else if constexpr (L == 7) return fe_m0_val_L7;
+  else return fe_m0_val_L8;
+}
+template <int L>
+FE_DEV const signed char* fe_m0_m() {
+  if constexpr (L == 0) return fe_m0_m_L0; else if constexpr (L == 1) return fe_m0_m_L1;
+  else if constexpr (L == 2) return fe_m0_m_L2; else if constexpr (L == 3) return fe_m0_m_L3;
+  else if constexpr (L == 4) return fe_m0_m_L4; else if constexpr (L == 5) return fe_m0_m_L5;
+  else if constexpr (L == 6) return fe_m0_m_L6; else if constexpr (L == 7) return fe_m0_m_L7;
+  else return fe_m0_m_L8;
+}
+
+// E[i][j][t] of (u + xa)^i (u + xb)^j exp(-p u^2), i <= LA, j <= LB, t <= LA+LB.
+template <int LA, int LB>
+FE_DEV void fe_hermite_1d(double ip, double xa, double xb,
+                          double (&e)[LA + 1][LB + 1][LA + LB + 1]) {
+  constexpr int TM = LA + LB;
+#pragma unroll
+  for (int i = 0; i <= LA; ++i)
+#pragma unroll
+    for (int j = 0; j <= LB; ++j)
+#pragma unroll
+      for (int t = 0; t <= TM; ++t) e[i][j][t] = 0.0;
+  e[0][0][0] = 1.0;
+#pragma unroll
+  for (int i = 0; i <= LA; ++i)
+#pragma unroll
+    for (int j = 0; j <= LB; ++j) {
+      if (i == 0 && j == 0) continue;
+      const int si = i > 0 ? i - 1 : i, sj = i > 0 ? j : j - 1;
+      const double x = i > 0 ? xa : xb;
+#pragma unroll
+      for (int t = 0; t <= TM; ++t) {
+        double v = 0.0;
+        if (t >= 1) v += e[si][sj][t - 1] * ip;
+        v += x * e[si][sj][t];
+        if (t + 1 <= TM) v += double(t + 1) * e[si][sj][t + 1];
+        e[i][j][t] = v;
+      }
+    }
+}
+
+template <int LA, int LB>
+FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
+  constexpr int L = LA + LB;
+  constexpr int NA = (LA + 1) * (LA + 2) / 2, NB = (LB + 1) * (LB + 2) / 2;
+  constexpr int NTRI = (L + 1) * (L + 2) * (L + 3) / 6;
+  constexpr int NT = fe_class_nterm[L];
+  constexpr int REC = fe_class_rec64[L];
+  const FeTask tk = a.tasks[a.work_task[w]];
+  const int ij = a.work_ij[w];
+  const int ii = ij >> 16, jj = ij & 0xffff;
+  const FeShell& A = a.shells[tk.si];
+  const FeShell& B = a.shells[tk.sj];
+  const long long slot = a.class_slot0[L] + tk.slot0 + ii * B.nprim + jj;
+  a.keep[slot] = 0;
+  a.srule[slot] = 0.0;
+
+  // density block of the shell pair (both orderings for si != sj)
+  double W[NA * NB];
+  double wmax = 0.0;
+#pragma unroll
+  for (int mu = 0; mu < NA; ++mu)
+#pragma unroll
+    for (int nu = 0; nu < NB; ++nu) {
+      double d = a.dens[size_t(A.fn0 + mu) * a.n_func + (B.fn0 + nu)];
+      if (tk.si != tk.sj) d += a.dens[size_t(B.fn0 + nu) * a.n_func + (A.fn0 + mu)];
+      W[mu * NB + nu] = d;
+      wmax = fmax(wmax, fabs(d));
+    }
+  if (!(wmax >= 1e-15)) return;
+
+  const double al = a.sexp[A.prim0 + ii], be = a.sexp[B.prim0 + jj];
+  const double cc = a.scoef[A.prim0 + ii] * a.scoef[B.prim0 + jj];
+  const double p = al + be;
+  double ab2 = 0.0, P[3], xa[3], xb[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double d = A.c[k] - B.c[k];
+    ab2 += d * d;
+  }
+  const double K = exp(-(al * be) / p * ab2);
+  if (!(K >= 1e-30)) return;
+  if (a.rule == 1 && cc == 0.0) return;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    P[k] = (al * A.c[k] + be * B.c[k]) / p;
+    xa[k] = P[k] - A.c[k];
+    xb[k] = P[k] - B.c[k];
+  }
+  const double ip = 1.0 / (2.0 * p);
+  double ex[LA + 1][LB + 1][L + 1], ey[LA + 1][LB + 1][L + 1], ez[LA + 1][LB + 1][L + 1];
+  fe_hermite_1d<LA, LB>(ip, xa[0], xb[0], ex);
+  fe_hermite_1d<LA, LB>(ip, xa[1], xb[1], ey);
+  fe_hermite_1d<LA, LB>(ip, xa[2], xb[2], ez);
+
+  double etab[NTRI];
+#pragma unroll
+  for (int t = 0; t < NTRI; ++t) etab[t] = 0.0;
+#pragma unroll 1
+  for (int mu = 0; mu < NA; ++mu) {
+    const int ax = fe_cart[LA][mu][0], ay = fe_cart[LA][mu][1], az = fe_cart[LA][mu][2];
+#pragma unroll 1
+    for (int nu = 0; nu < NB; ++nu) {
+      const double wt = W[mu * NB + nu] * cc;
+      if (wt == 0.0) continue;
+      const int bx = fe_cart[LB][nu][0], by = fe_cart[LB][nu][1], bz = fe_cart[LB][nu][2];
+      for (int tx = 0; tx <= ax + bx; ++tx) {
+        const double vx = wt * ex[ax][bx][tx];
+        for (int ty = 0; ty <= ay + by; ++ty) {
+          const double vxy = vx * ey[ay][by][ty];
+          const int base = fe_tri<L>(tx, ty, 0);
+          for (int tz = 0; tz <= az + bz; ++tz) etab[base + tz] += vxy * ez[az][bz][tz];
+        }
+      }
+    }
+  }
+  // sum rule: int rho_pair = K (pi/p)^1.5 etab[0]   (build_pairs.cpp:294-296)
+  a.srule[slot] = K * pow(3.14159265358979323846 / p, 1.5) * etab[0];
+
+  // G_k = (2 pi / p) (2p)^m_k sum_t M0[k,t] etab[t]
+  const double cf = 2.0 * 3.14159265358979323846 / p;
+  const double tp = 2.0 * p;
+  double pw[L + 1];
+  pw[0] = 1.0;
+#pragma unroll
+  for (int m = 1; m <= L; ++m) pw[m] = pw[m - 1] * tp;
+  double* rec = a.stage + a.stage_off[L] + (slot - a.class_slot0[L]) * REC;
+  const short* rp = fe_m0_ptr<L>();
+  const short* rc = fe_m0_col<L>();
+  const float* rv = fe_m0_val<L>();
+  const signed char* rm = fe_m0_m<L>();
+  bool anyg = false;
+#pragma unroll 1
+  for (int k = 0; k < NT; ++k) {
+    double s = 0.0;
+    for (int q = rp[k]; q < rp[k + 1]; ++q) s += double(rv[q]) * etab[rc[q]];
+    const double g = cf * pw[rm[k]] * s;
+    anyg |= (g != 0.0);
+    rec[5 + k] = g;
+  }
+  if (a.rule == 1 && !anyg) return;
+
+  // screening bound (esp.py:251-254)
+  const double sq = sqrt(tp);
+  double sqp[L + 1];
+  sqp[0] = 1.0;
+#pragma unroll
+  for (int m = 1; m <= L; ++m) sqp[m] = sqp[m - 1] * sq;
+  double bsum = 0.0;
+#pragma unroll
+  for (int tx = 0; tx <= L; ++tx)
+#pragma unroll
+    for (int ty = 0; ty <= L - tx; ++ty)
+#pragma unroll
+      for (int tz = 0; tz <= L - tx - ty; ++tz)
+        bsum += fabs(etab[fe_tri<L>(tx, ty, tz)]) * (fe_screen_mom[tx] * fe_screen_mom[ty]
+                 * fe_screen_mom[tz]) * sqp[tx + ty + tz];
+  const double bound = pow(tp, -1.5) * bsum;
+  const double reff = 1.6 * sqrt((L + 2.0) / p);
+
+  // nearest point (exact IEEE arithmetic, no contraction, as NumPy does)
+  double d2min = 1e300;
+  for (int q = 0; q < a.npts; ++q) {
+    const double dx = __dsub_rn(a.pts[3 * q], P[0]);
+    const double dy = __dsub_rn(a.pts[3 * q + 1], P[1]);
+    const double dz = __dsub_rn(a.pts[3 * q + 2], P[2]);
+    const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+    d2min = fmin(d2min, d2);
+  }
+  double dd = __dsqrt_rn(d2min);
+  if (a.rule == 1) dd = dd - reff;
+  dd = fmax(dd, 0.05);
+  const bool keep = a.npts == 0 ? true : !(__ddiv_rn(__dmul_rn(K, bound), dd) < a.tol);
+  if (!keep) return;
+  rec[0] = p;
+  rec[1] = P[0];
+  rec[2] = P[1];
+  rec[3] = P[2];
+  rec[4] = K;
+#pragma unroll
+  for (int k = 5 + NT; k < REC; ++k) rec[k] = 0.0;
+  a.keep[slot] = 1;
+}
+
+#define FE_BUILD_THREADS 128
+
+__global__ void __launch_bounds__(FE_BUILD_THREADS) fe_build_kernel(const FeBuildArgs a) {
+  int g = 0;
+  while (g + 1 < a.ngroup && int(blockIdx.x) >= a.grp_block0[g + 1]) ++g;
+  const int w = (blockIdx.x - a.grp_block0[g]) * FE_BUILD_THREADS + threadIdx.x;
+  if (w >= a.grp_nwork[g]) return;
+  const int wi = a.grp_work0[g] + w;
+  switch (a.grp_code[g]) {
+#define FE_CASE(la, lb) case la * 5 + lb: fe_build_pair<la, lb>(a, wi); break;
+    FE_CASE(0, 0) FE_CASE(0, 1) FE_CASE(0, 2) FE_CASE(0, 3) FE_CASE(0, 4)
+    FE_CASE(1, 0) FE_CASE(1, 1) FE_CASE(1, 2) FE_CASE(1, 3) FE_CASE(1, 4)
+    FE_CASE(2, 0) FE_CASE(2, 1) FE_CASE(2, 2) FE_CASE(2, 3) FE_CASE(2, 4)
+    FE_CASE(3, 0) FE_CASE(3, 1) FE_CASE(3, 2) FE_CASE(3, 3) FE_CASE(3, 4)
+    FE_CASE(4, 0) FE_CASE(4, 1) FE_CASE(4, 2) FE_CASE(4, 3) FE_CASE(4, 4)
+#undef FE_CASE
+    default: fe_flag(FE_ST_BADCLASS); break;
+  }
+}
+
+// Move kept staging records of every class, in slot order, into the table.
+// ``pos`` is the exclusive scan of ``keep`` over all global slots.
+__global__ void fe_scatter_kernel(const double* __restrict__ stage, const long long* stage_off,
+                                  const long long* class_slot0, int nclass,
+                                  const int* __restrict__ keep, const int* __restrict__ pos,
+                                  long long nslot, unsigned char* table) {
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= nslot || !keep[s]) return;
+  int L = 0;
+  while (L + 1 < nclass && s >= class_slot0[L + 1]) ++L;
+  const FeTableHdr* hdr = reinterpret_cast<const FeTableHdr*>(table);
+  const int dst = pos[s] - pos[class_slot0[L]];
+  if (dst >= hdr->cap[L]) { fe_flag(FE_ST_OVERFLOW); return; }
+  const int R = fe_c_rec64[L];
+  const double* src = stage + stage_off[L] + (s - class_slot0[L]) * R;
+  double* out = reinterpret_cast<double*>(table + hdr->off64[L]) + size_t(dst) * R;
+  for (int k = 0; k < R; ++k) out[k] = src[k];
+}
+
+// Per-class kept counts and the sum rule.  One block of 1024 threads: each
+// thread sums a fixed strided subset of slots, then a fixed-shape tree adds
+// the partial sums, so the result does not depend on scheduling.
+__global__ void __launch_bounds__(1024) fe_finalize_kernel(
+    const long long* class_slot0, int nclass, long long nslot, const int* __restrict__ keep,
+    const int* __restrict__ pos, const double* __restrict__ srule, unsigned char* table) {
+  __shared__ double red[1024];
+  FeTableHdr* hdr = reinterpret_cast<FeTableHdr*>(table);
+  const int t = threadIdx.x;
+  if (t < nclass) {
+    const long long a0 = class_slot0[t], a1 = class_slot0[t + 1];
+    hdr->count[t] = a1 > a0 ? pos[a1 - 1] + keep[a1 - 1] - pos[a0] : 0;
+  }
+  double s = 0.0;
+  for (long long q = t; q < nslot; q += 1024) s += srule[q];
+  red[t] = s;
+  __syncthreads();
+  for (int h = 512; h > 0; h >>= 1) {
+    if (t < h) red[t] += red[t + h];
+    __syncthreads();
+  }
+  if (t == 0) hdr->sum_rule = red[0];
+}
+
+// Exclusive scan of the keep flags in three deterministic passes:
+// per-block sums, a single-block scan of those sums, then per-block scans.
+#define FE_SCAN_BLOCK 1024
+
+__global__ void __launch_bounds__(FE_SCAN_BLOCK) fe_scan_sums_kernel(
+    const int* __restrict__ keep, long long n, int* __restrict__ bsum) {
+  __shared__ int red[FE_SCAN_BLOCK];
+  const long long i = blockIdx.x * (long long)FE_SCAN_BLOCK + threadIdx.x;
+  red[threadIdx.x] = i < n ? keep[i] : 0;
+  __syncthreads();
+  for (int h = FE_SCAN_BLOCK / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) bsum[blockIdx.x] = red[0];
+}
+
+// In-place exclusive scan of ``bsum`` (nb entries) by one block.
+__global__ void __launch_bounds__(FE_SCAN_BLOCK) fe_scan_top_kernel(int* bsum, int nb) {
+  __shared__ int buf[FE_SCAN_BLOCK];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nb; base += FE_SCAN_BLOCK) {
+    const int i = base + threadIdx.x;
+    const int v = i < nb ? bsum[i] : 0;
+    buf[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = 1; off < FE_SCAN_BLOCK; off <<= 1) {   // Hillis-Steele inclusive scan
+      const int add = threadIdx.x >= off ? buf[threadIdx.x - off] : 0;
+      __syncthreads();
+      buf[threadIdx.x] += add;
+      __syncthreads();
+    }
+    if (i < nb) bsum[i] = carry + buf[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == FE_SCAN_BLOCK - 1) carry += buf[FE_SCAN_BLOCK - 1];
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(FE_SCAN_BLOCK) fe_scan_apply_kernel(
+    const int* __restrict__ keep, long long n, const int* __restrict__ bsum, int* __restrict__ pos) {
+  __shared__ int buf[FE_SCAN_BLOCK];
+  const long long i = blockIdx.x * (long long)FE_SCAN_BLOCK + threadIdx.x;
+  const int v = i < n ? keep[i] : 0;
+  buf[threadIdx.x] = v;
+  __syncthreads();
+  for (int off = 1; off < FE_SCAN_BLOCK; off <<= 1) {
+    const int add = threadIdx.x >= off ? buf[threadIdx.x - off] : 0;
+    __syncthreads();
+    buf[threadIdx.x] += add;
+    __syncthreads();
+  }
+  if (i < n) pos[i] = bsum[blockIdx.x] + buf[threadIdx.x] - v;
+}
+
+// FP32 records of the mixed-precision path from the FP64 records.
+__global__ void fe_make_f32_kernel(unsigned char* table) {
+  FeTableHdr* hdr = reinterpret_cast<FeTableHdr*>(table);
+  const int L = blockIdx.y;
+  const int n = hdr->count[L];
+  const int R64 = fe_c_rec64[L], R32 = fe_c_rec32[L], NT = fe_c_nterm[L];
+  const double* src = reinterpret_cast<const double*>(table + hdr->off64[L]);
+  float* dst = reinterpret_cast<float*>(table + hdr->off32[L]);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double* r = src + size_t(i) * R64;
+    float* o = dst + size_t(i) * R32;
+    o[0] = float(r[0]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float hi = float(r[1 + k]);
+      o[1 + k] = hi;
+      o[4 + k] = float(r[1 + k] - double(hi));
+    }
+    o[7] = float(r[4]);
+    for (int k = 0; k < NT; ++k) o[8 + k] = float(r[5 + k]);
+    for (int k = 8 + NT; k < R32; ++k) o[k] = 0.0f;
+  }
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) hdr->has32 = 1;
+}

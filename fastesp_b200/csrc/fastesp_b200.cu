@@ -1,0 +1,584 @@
+// libfastesp_b200: the C ABI of include/fastesp_b200.h.
+//
+// Single translation unit: the device code lives in the included headers,
+// this file holds the host-side planning and the extern "C" entry points.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstddef>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "classes_gen.cuh"
+#include "boys.cuh"
+#include "table.cuh"
+#include "eval_f64.cuh"
+#include "build.cuh"
+#include "../../include/fastesp_b200.h"
+
+static_assert(FE_NCLASS <= FE_NCLASS_MAX, "class count");
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define FE_CUDA(call)                                                              \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess)                                                         \
+      return fail(FE_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_),     \
+                  __FILE__, __LINE__);                                             \
+  } while (0)
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+int sm_count() {
+  int dev = 0, n = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n > 0 ? n : 148;
+}
+
+// ---------------------------------------------------------------------------
+// Evaluation launch geometry
+// ---------------------------------------------------------------------------
+constexpr int kEvalThreads = 128;
+constexpr int kEvalNP = 2;
+
+struct EvalGeom {
+  int nblk_x, nsplit, ld;
+};
+
+EvalGeom eval_geom(int npts, int pts_per_block) {
+  EvalGeom g;
+  g.nblk_x = (npts + pts_per_block - 1) / pts_per_block;
+  const int target = 3 * sm_count();
+  g.nsplit = std::max(1, std::min(256, (target + g.nblk_x - 1) / std::max(1, g.nblk_x)));
+  g.ld = (npts + 31) & ~31;
+  return g;
+}
+
+struct Layout {
+  size_t off64[FE_NCLASS], off32[FE_NCLASS], off_atoms, bytes;
+};
+
+Layout table_layout(const int* cap, int n_atoms) {
+  Layout l{};
+  size_t t = FE_TABLE_HDR_BYTES;
+  for (int L = 0; L < FE_NCLASS; ++L) {
+    l.off64[L] = t;
+    t = align256(t + size_t(cap[L]) * fe_class_rec64[L] * 8);
+  }
+  for (int L = 0; L < FE_NCLASS; ++L) {
+    l.off32[L] = t;
+    t = align256(t + size_t(cap[L]) * fe_class_rec32[L] * 4);
+  }
+  l.off_atoms = t;
+  l.bytes = align256(t + size_t(n_atoms) * 4 * sizeof(double));
+  return l;
+}
+
+// Header + atom block of a table with the given capacities (counts zero).
+int write_header(unsigned char* d_table, const int* cap, int n_atoms, const double* Z,
+                 const double* xyz, double tol, int rule, cudaStream_t st) {
+  const Layout lay = table_layout(cap, n_atoms);
+  FeTableHdr hdr{};
+  hdr.magic = FE_TABLE_MAGIC;
+  hdr.nclass = FE_NCLASS;
+  hdr.n_atoms = n_atoms;
+  hdr.rule = rule;
+  hdr.tol = tol;
+  for (int L = 0; L < FE_NCLASS; ++L) {
+    hdr.cap[L] = cap[L];
+    hdr.off64[L] = static_cast<long long>(lay.off64[L]);
+    hdr.off32[L] = static_cast<long long>(lay.off32[L]);
+  }
+  hdr.off_atoms = static_cast<long long>(lay.off_atoms);
+  hdr.bytes = static_cast<long long>(lay.bytes);
+  std::vector<unsigned char> h(sizeof hdr + size_t(n_atoms) * 4 * sizeof(double));
+  memcpy(h.data(), &hdr, sizeof hdr);
+  FE_CUDA(cudaMemcpyAsync(d_table, h.data(), sizeof hdr, cudaMemcpyHostToDevice, st));
+  if (n_atoms > 0) {
+    std::vector<double> atoms(Z, Z + n_atoms);
+    atoms.insert(atoms.end(), xyz, xyz + 3 * size_t(n_atoms));
+    FE_CUDA(cudaMemcpyAsync(d_table + lay.off_atoms, atoms.data(), atoms.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, st));
+  }
+  FE_CUDA(cudaStreamSynchronize(st));   // host staging buffers are locals
+  return FE_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Plan
+// ---------------------------------------------------------------------------
+struct fe_plan {
+  int n_func = 0, n_atoms = 0;
+  std::vector<FeShell> shells;
+  std::vector<double> sexp, scoef;
+  std::vector<FeTask> tasks;
+  std::vector<int> work_task, work_ij;
+  std::vector<int> grp_block0, grp_code, grp_work0, grp_nwork;
+  std::vector<long long> class_slot0;   // FE_NCLASS + 1
+  std::vector<long long> stage_off;     // FE_NCLASS, in doubles
+  std::vector<double> Z, xyz;
+  long long nslot = 0;
+  int nblocks = 0;
+  int cap[FE_NCLASS] = {};
+  // device blob layout (byte offsets)
+  size_t o_shells, o_sexp, o_scoef, o_tasks, o_wt, o_wij, o_gb, o_gc, o_gw, o_gn, o_cs, o_so;
+  size_t plan_bytes = 0;
+  size_t table_bytes = 0;
+  size_t o_tab64[FE_NCLASS], o_tab32[FE_NCLASS], o_atoms = 0;
+  size_t ws_stage = 0, ws_keep = 0, ws_pos = 0, ws_srule = 0, ws_bsum = 0;
+  long long nscan_blocks = 0;
+  size_t ws_bytes = 0;
+};
+
+extern "C" {
+
+int fe_version(void) { return 100; }
+
+const char* fe_last_error(void) { return g_err.c_str(); }
+
+int fe_status(unsigned* bits, int clear) {
+  FE_CUDA(cudaDeviceSynchronize());
+  unsigned v = 0;
+  FE_CUDA(cudaMemcpyFromSymbol(&v, fe_status_word, sizeof v));
+  if (clear) {
+    const unsigned z = 0;
+    FE_CUDA(cudaMemcpyToSymbol(fe_status_word, &z, sizeof z));
+  }
+  if (bits) *bits = v;
+  return FE_OK;
+}
+
+int fe_plan_create(const fe_basis* b, fe_plan** out) {
+  if (!b || !out) return fail(FE_ERR_ARG, "fe_plan_create: null argument");
+  *out = nullptr;
+  if (b->n_func < 0 || b->n_prim < 0 || b->n_atoms < 0)
+    return fail(FE_ERR_ARG, "fe_plan_create: negative size");
+  auto* p = new fe_plan();
+  p->n_func = b->n_func;
+  p->n_atoms = b->n_atoms;
+  p->Z.assign(b->Z, b->Z + b->n_atoms);
+  p->xyz.assign(b->xyz, b->xyz + 3 * size_t(b->n_atoms));
+  // shells = contiguous runs of equal fn_shell (build_pairs.cpp:170-182)
+  for (int i = 0; i < b->n_func;) {
+    int j = i;
+    while (j < b->n_func && b->fn_shell[j] == b->fn_shell[i]) ++j;
+    FeShell s{};
+    s.atom = b->fn_atom[i];
+    s.l = b->fn_lx[i] + b->fn_ly[i] + b->fn_lz[i];
+    s.fn0 = i;
+    s.nprim = b->fn_nprim[i];
+    const int nc = (s.l + 1) * (s.l + 2) / 2;
+    if (s.l > 4) { delete p; return fail(FE_ERR_UNSUPPORTED, "shell %zu has l=%d > 4", p->shells.size(), s.l); }
+    if (j - i != nc) { delete p; return fail(FE_ERR_ARG, "shell at function %d has %d functions, expected %d", i, j - i, nc); }
+    if (s.nprim <= 0 || s.nprim > 65535 || b->fn_off[i] < 0 || b->fn_off[i] + s.nprim > b->n_prim) {
+      delete p; return fail(FE_ERR_ARG, "shell at function %d: bad primitive range", i);
+    }
+    if (s.atom < 0 || s.atom >= b->n_atoms) { delete p; return fail(FE_ERR_ARG, "function %d: atom out of range", i); }
+    s.prim0 = int(p->sexp.size());
+    for (int k = 0; k < s.nprim; ++k) {
+      p->sexp.push_back(b->pexp[b->fn_off[i] + k]);
+      p->scoef.push_back(b->pcoef[b->fn_off[i] + k]);
+    }
+    for (int k = 0; k < 3; ++k) s.c[k] = b->fc[3 * size_t(i) + k];
+    p->shells.push_back(s);
+    i = j;
+  }
+  const int ns = int(p->shells.size());
+  // shell pairs in reference order, class slot numbering per class
+  long long cls_count[FE_NCLASS] = {};
+  std::vector<std::vector<int>> grp_tasks(25);
+  for (int si = 0; si < ns; ++si)
+    for (int sj = si; sj < ns; ++sj) {
+      const FeShell& A = p->shells[si];
+      const FeShell& B = p->shells[sj];
+      const int L = A.l + B.l;
+      FeTask t{};
+      t.si = si;
+      t.sj = sj;
+      t.slot0 = int(cls_count[L]);
+      cls_count[L] += (long long)A.nprim * B.nprim;
+      if (cls_count[L] > (1LL << 30)) { delete p; return fail(FE_ERR_SIZE, "class %d too large", L); }
+      grp_tasks[A.l * 5 + B.l].push_back(int(p->tasks.size()));
+      p->tasks.push_back(t);
+    }
+  p->class_slot0.assign(FE_NCLASS + 1, 0);
+  p->stage_off.assign(FE_NCLASS, 0);
+  long long so = 0;
+  for (int L = 0; L < FE_NCLASS; ++L) {
+    p->class_slot0[L + 1] = p->class_slot0[L] + cls_count[L];
+    p->cap[L] = int(cls_count[L]);
+    p->stage_off[L] = so;
+    so += cls_count[L] * fe_class_rec64[L];
+  }
+  p->nslot = p->class_slot0[FE_NCLASS];
+  int block = 0;
+  for (int code = 0; code < 25; ++code) {
+    if (grp_tasks[code].empty()) continue;
+    const int w0 = int(p->work_task.size());
+    for (int ti : grp_tasks[code]) {
+      const FeTask& t = p->tasks[ti];
+      const int na = p->shells[t.si].nprim, nb = p->shells[t.sj].nprim;
+      for (int i = 0; i < na; ++i)
+        for (int j = 0; j < nb; ++j) {
+          p->work_task.push_back(ti);
+          p->work_ij.push_back((i << 16) | j);
+        }
+    }
+    const int nw = int(p->work_task.size()) - w0;
+    if (nw == 0) continue;
+    p->grp_block0.push_back(block);
+    p->grp_code.push_back(code);
+    p->grp_work0.push_back(w0);
+    p->grp_nwork.push_back(nw);
+    block += (nw + FE_BUILD_THREADS - 1) / FE_BUILD_THREADS;
+  }
+  p->nblocks = block;
+  // device plan blob
+  size_t o = 0;
+  auto put = [&](size_t bytes) { const size_t at = o; o = align256(o + bytes); return at; };
+  p->o_shells = put(sizeof(FeShell) * p->shells.size());
+  p->o_sexp = put(sizeof(double) * p->sexp.size());
+  p->o_scoef = put(sizeof(double) * p->scoef.size());
+  p->o_tasks = put(sizeof(FeTask) * p->tasks.size());
+  p->o_wt = put(sizeof(int) * p->work_task.size());
+  p->o_wij = put(sizeof(int) * p->work_ij.size());
+  p->o_gb = put(sizeof(int) * p->grp_block0.size());
+  p->o_gc = put(sizeof(int) * p->grp_code.size());
+  p->o_gw = put(sizeof(int) * p->grp_work0.size());
+  p->o_gn = put(sizeof(int) * p->grp_nwork.size());
+  p->o_cs = put(sizeof(long long) * p->class_slot0.size());
+  p->o_so = put(sizeof(long long) * p->stage_off.size());
+  p->plan_bytes = std::max<size_t>(o, 256);
+  // table layout
+  {
+    const Layout lay = table_layout(p->cap, p->n_atoms);
+    for (int L = 0; L < FE_NCLASS; ++L) {
+      p->o_tab64[L] = lay.off64[L];
+      p->o_tab32[L] = lay.off32[L];
+    }
+    p->o_atoms = lay.off_atoms;
+    p->table_bytes = lay.bytes;
+  }
+  // build workspace
+  size_t w = 0;
+  auto wput = [&](size_t bytes) { const size_t at = w; w = align256(w + bytes); return at; };
+  p->ws_stage = wput(size_t(so) * sizeof(double));
+  p->ws_keep = wput(size_t(p->nslot + 1) * sizeof(int));
+  p->ws_pos = wput(size_t(p->nslot + 1) * sizeof(int));
+  p->ws_srule = wput(size_t(p->nslot + 1) * sizeof(double));
+  p->nscan_blocks = (p->nslot + FE_SCAN_BLOCK - 1) / FE_SCAN_BLOCK;
+  p->ws_bsum = wput(size_t(p->nscan_blocks + 1) * sizeof(int));
+  p->ws_bytes = std::max<size_t>(w, 256);
+  *out = p;
+  return FE_OK;
+}
+
+void fe_plan_destroy(fe_plan* plan) { delete plan; }
+
+int fe_plan_sizes(const fe_plan* p, fe_sizes* s) {
+  if (!p || !s) return fail(FE_ERR_ARG, "fe_plan_sizes: null argument");
+  s->plan_bytes = p->plan_bytes;
+  s->table_bytes = p->table_bytes;
+  s->build_ws_bytes = p->ws_bytes;
+  s->n_shell = int(p->shells.size());
+  s->n_shell_pair = int(p->tasks.size());
+  s->n_work = int(p->work_task.size());
+  for (int L = 0; L < FE_NCLASS; ++L) s->cap[L] = p->cap[L];
+  return FE_OK;
+}
+
+int fe_plan_upload(const fe_plan* p, void* d_plan, cudaStream_t st) {
+  if (!p || !d_plan) return fail(FE_ERR_ARG, "fe_plan_upload: null argument");
+  if (reinterpret_cast<uintptr_t>(d_plan) & 255) return fail(FE_ERR_ARG, "fe_plan_upload: buffer not 256-byte aligned");
+  std::vector<unsigned char> h(p->plan_bytes, 0);
+  auto cp = [&](size_t off, const void* src, size_t bytes) { if (bytes) memcpy(h.data() + off, src, bytes); };
+  cp(p->o_shells, p->shells.data(), sizeof(FeShell) * p->shells.size());
+  cp(p->o_sexp, p->sexp.data(), sizeof(double) * p->sexp.size());
+  cp(p->o_scoef, p->scoef.data(), sizeof(double) * p->scoef.size());
+  cp(p->o_tasks, p->tasks.data(), sizeof(FeTask) * p->tasks.size());
+  cp(p->o_wt, p->work_task.data(), sizeof(int) * p->work_task.size());
+  cp(p->o_wij, p->work_ij.data(), sizeof(int) * p->work_ij.size());
+  cp(p->o_gb, p->grp_block0.data(), sizeof(int) * p->grp_block0.size());
+  cp(p->o_gc, p->grp_code.data(), sizeof(int) * p->grp_code.size());
+  cp(p->o_gw, p->grp_work0.data(), sizeof(int) * p->grp_work0.size());
+  cp(p->o_gn, p->grp_nwork.data(), sizeof(int) * p->grp_nwork.size());
+  cp(p->o_cs, p->class_slot0.data(), sizeof(long long) * p->class_slot0.size());
+  cp(p->o_so, p->stage_off.data(), sizeof(long long) * p->stage_off.size());
+  FE_CUDA(cudaMemcpyAsync(d_plan, h.data(), h.size(), cudaMemcpyHostToDevice, st));
+  FE_CUDA(cudaStreamSynchronize(st));   // h is a local buffer
+  return FE_OK;
+}
+
+int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
+                   const double* d_pts, int n_pts, double tol, int rule, void* d_table,
+                   void* d_ws, size_t ws_bytes, cudaStream_t st) {
+  if (!p || !d_plan || !d_table || !d_ws || (p->n_func && !d_dens))
+    return fail(FE_ERR_ARG, "fe_table_build: null argument");
+  if (n_pts < 0 || (n_pts > 0 && !d_pts)) return fail(FE_ERR_ARG, "fe_table_build: bad points");
+  if (rule != FE_RULE_NUMPY && rule != FE_RULE_NATIVE) return fail(FE_ERR_ARG, "fe_table_build: unknown rule %d", rule);
+  if (!(tol >= 0.0)) return fail(FE_ERR_ARG, "fe_table_build: tol must be >= 0");
+  if (ws_bytes < p->ws_bytes) return fail(FE_ERR_SIZE, "fe_table_build: workspace %zu < %zu bytes", ws_bytes, p->ws_bytes);
+  if ((reinterpret_cast<uintptr_t>(d_table) | reinterpret_cast<uintptr_t>(d_ws) |
+       reinterpret_cast<uintptr_t>(d_plan)) & 255)
+    return fail(FE_ERR_ARG, "fe_table_build: buffers must be 256-byte aligned");
+  const unsigned char* pb = static_cast<const unsigned char*>(d_plan);
+  unsigned char* wb = static_cast<unsigned char*>(d_ws);
+  unsigned char* tb = static_cast<unsigned char*>(d_table);
+  {
+    const int rc = write_header(tb, p->cap, p->n_atoms, p->Z.data(), p->xyz.data(), tol, rule, st);
+    if (rc != FE_OK) return rc;
+  }
+  FeBuildArgs a{};
+  a.shells = reinterpret_cast<const FeShell*>(pb + p->o_shells);
+  a.sexp = reinterpret_cast<const double*>(pb + p->o_sexp);
+  a.scoef = reinterpret_cast<const double*>(pb + p->o_scoef);
+  a.tasks = reinterpret_cast<const FeTask*>(pb + p->o_tasks);
+  a.work_task = reinterpret_cast<const int*>(pb + p->o_wt);
+  a.work_ij = reinterpret_cast<const int*>(pb + p->o_wij);
+  a.grp_block0 = reinterpret_cast<const int*>(pb + p->o_gb);
+  a.grp_code = reinterpret_cast<const int*>(pb + p->o_gc);
+  a.grp_work0 = reinterpret_cast<const int*>(pb + p->o_gw);
+  a.grp_nwork = reinterpret_cast<const int*>(pb + p->o_gn);
+  a.ngroup = int(p->grp_code.size());
+  a.n_func = p->n_func;
+  a.dens = d_dens;
+  a.pts = d_pts;
+  a.npts = n_pts;
+  a.tol = tol;
+  a.rule = rule;
+  a.class_slot0 = reinterpret_cast<const long long*>(pb + p->o_cs);
+  a.stage = reinterpret_cast<double*>(wb + p->ws_stage);
+  a.stage_off = reinterpret_cast<const long long*>(pb + p->o_so);
+  a.keep = reinterpret_cast<int*>(wb + p->ws_keep);
+  a.srule = reinterpret_cast<double*>(wb + p->ws_srule);
+  if (p->nblocks > 0) {
+    fe_build_kernel<<<p->nblocks, FE_BUILD_THREADS, 0, st>>>(a);
+    FE_CUDA(cudaGetLastError());
+  }
+  int* pos = reinterpret_cast<int*>(wb + p->ws_pos);
+  if (p->nslot > 0) {
+    int* bsum = reinterpret_cast<int*>(wb + p->ws_bsum);
+    const unsigned nb = unsigned(p->nscan_blocks);
+    fe_scan_sums_kernel<<<nb, FE_SCAN_BLOCK, 0, st>>>(a.keep, p->nslot, bsum);
+    fe_scan_top_kernel<<<1, FE_SCAN_BLOCK, 0, st>>>(bsum, int(nb));
+    fe_scan_apply_kernel<<<nb, FE_SCAN_BLOCK, 0, st>>>(a.keep, p->nslot, bsum, pos);
+    FE_CUDA(cudaGetLastError());
+    const int thr = 256;
+    fe_scatter_kernel<<<unsigned((p->nslot + thr - 1) / thr), thr, 0, st>>>(
+        a.stage, a.stage_off, a.class_slot0, FE_NCLASS, a.keep, pos, p->nslot, tb);
+    FE_CUDA(cudaGetLastError());
+  }
+  fe_finalize_kernel<<<1, 1024, 0, st>>>(a.class_slot0, FE_NCLASS, p->nslot, a.keep, pos, a.srule, tb);
+  FE_CUDA(cudaGetLastError());
+  fe_make_f32_kernel<<<dim3(std::max(1, 2 * sm_count() / FE_NCLASS), FE_NCLASS), 256, 0, st>>>(tb);
+  FE_CUDA(cudaGetLastError());
+  return FE_OK;
+}
+
+size_t fe_table_bytes(const int* cap, int n_atoms) {
+  if (!cap || n_atoms < 0) return 0;
+  for (int L = 0; L < FE_NCLASS; ++L)
+    if (cap[L] < 0) return 0;
+  return table_layout(cap, n_atoms).bytes;
+}
+
+int fe_table_offsets(const int* cap, int n_atoms, size_t* off64, size_t* off32, size_t* off_atoms) {
+  if (!cap || n_atoms < 0) return fail(FE_ERR_ARG, "fe_table_offsets: bad argument");
+  const Layout lay = table_layout(cap, n_atoms);
+  for (int L = 0; L < FE_NCLASS; ++L) {
+    if (off64) off64[L] = lay.off64[L];
+    if (off32) off32[L] = lay.off32[L];
+  }
+  if (off_atoms) *off_atoms = lay.off_atoms;
+  return FE_OK;
+}
+
+int fe_table_init(void* d_table, const int* count, int n_atoms, const double* Z,
+                  const double* xyz, cudaStream_t st) {
+  if (!d_table || !count || n_atoms < 0 || (n_atoms > 0 && (!Z || !xyz)))
+    return fail(FE_ERR_ARG, "fe_table_init: bad argument");
+  if (reinterpret_cast<uintptr_t>(d_table) & 255) return fail(FE_ERR_ARG, "fe_table_init: buffer not 256-byte aligned");
+  unsigned char* tb = static_cast<unsigned char*>(d_table);
+  const int rc = write_header(tb, count, n_atoms, Z, xyz, 0.0, -1, st);
+  if (rc != FE_OK) return rc;
+  // counts equal capacities for an imported table
+  FE_CUDA(cudaMemcpyAsync(tb + offsetof(FeTableHdr, count), count, sizeof(int) * FE_NCLASS,
+                          cudaMemcpyHostToDevice, st));
+  FE_CUDA(cudaStreamSynchronize(st));
+  return FE_OK;
+}
+
+int fe_table_make_f32(void* d_table, cudaStream_t st) {
+  if (!d_table) return fail(FE_ERR_ARG, "fe_table_make_f32: null table");
+  fe_make_f32_kernel<<<dim3(std::max(1, 2 * sm_count() / FE_NCLASS), FE_NCLASS), 256, 0, st>>>(
+      static_cast<unsigned char*>(d_table));
+  FE_CUDA(cudaGetLastError());
+  return FE_OK;
+}
+
+int fe_table_info_get(const void* d_table, fe_table_info* info, cudaStream_t st) {
+  if (!d_table || !info) return fail(FE_ERR_ARG, "fe_table_info_get: null argument");
+  FeTableHdr h{};
+  FE_CUDA(cudaMemcpyAsync(&h, d_table, sizeof h, cudaMemcpyDeviceToHost, st));
+  FE_CUDA(cudaStreamSynchronize(st));
+  if (h.magic != FE_TABLE_MAGIC) return fail(FE_ERR_ARG, "fe_table_info_get: not a pair table");
+  info->n_pairs = 0;
+  for (int L = 0; L < FE_NCLASS; ++L) {
+    info->count[L] = h.count[L];
+    info->n_pairs += h.count[L];
+  }
+  info->n_atoms = h.n_atoms;
+  info->sum_rule = h.sum_rule;
+  info->tol = h.tol;
+  info->rule = h.rule;
+  info->has_f32 = h.has32;
+  return FE_OK;
+}
+
+size_t fe_eval_ws_bytes(int n_pts, int mode) {
+  if (n_pts <= 0) return 256;
+  (void)mode;
+  const EvalGeom g = eval_geom(n_pts, kEvalThreads * kEvalNP);
+  return g.nsplit > 1 ? align256(size_t(g.nsplit) * g.ld * sizeof(double)) : 256;
+}
+
+}  // extern "C"
+
+namespace {
+
+int eval_f64(const char* who, const void* d_table, const double* d_pts, int n_pts,
+             double* d_out, void* d_ws, size_t ws_bytes, int mode, cudaStream_t st) {
+  if (n_pts < 0) return fail(FE_ERR_ARG, "%s: n_pts < 0", who);
+  if (n_pts == 0) return FE_OK;
+  if (!d_table || !d_pts || !d_out) return fail(FE_ERR_ARG, "%s: null argument", who);
+  const EvalGeom g = eval_geom(n_pts, kEvalThreads * kEvalNP);
+  if (g.nsplit > 1 && (!d_ws || ws_bytes < size_t(g.nsplit) * g.ld * sizeof(double)))
+    return fail(FE_ERR_SIZE, "%s: workspace too small (need %zu bytes)", who,
+                fe_eval_ws_bytes(n_pts, 0));
+  FeEvalArgs a{};
+  a.table = static_cast<const unsigned char*>(d_table);
+  a.pts = d_pts;
+  a.npts = n_pts;
+  a.nsplit = g.nsplit;
+  a.partial = static_cast<double*>(d_ws);
+  a.ld = g.ld;
+  a.out = d_out;
+  a.mode = mode;
+  const int smem = FE_NSTAGE * FE_STAGE_BYTES;
+  FE_CUDA(cudaFuncSetAttribute(fe_eval_f64_kernel<kEvalNP, kEvalThreads>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  fe_eval_f64_kernel<kEvalNP, kEvalThreads><<<dim3(g.nblk_x, g.nsplit), kEvalThreads, smem, st>>>(a);
+  FE_CUDA(cudaGetLastError());
+  if (g.nsplit > 1) {
+    fe_reduce_kernel<<<(n_pts + 255) / 256, 256, 0, st>>>(a.table, d_pts, n_pts, a.partial,
+                                                          g.nsplit, g.ld, d_out, mode);
+    FE_CUDA(cudaGetLastError());
+  }
+  return FE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fe_esp_fp64(const void* d_table, const double* d_pts, int n_pts, double* d_out,
+                void* d_ws, size_t ws_bytes, cudaStream_t st) {
+  return eval_f64("fe_esp_fp64", d_table, d_pts, n_pts, d_out, d_ws, ws_bytes, 0, st);
+}
+
+int fe_electron_fp64(const void* d_table, const double* d_pts, int n_pts, double* d_out,
+                     void* d_ws, size_t ws_bytes, cudaStream_t st) {
+  return eval_f64("fe_electron_fp64", d_table, d_pts, n_pts, d_out, d_ws, ws_bytes, 1, st);
+}
+
+int fe_nuclear_fp64(const void* d_table, const double* d_pts, int n_pts, double* d_out,
+                    void* d_ws, size_t ws_bytes, cudaStream_t st) {
+  (void)d_ws;
+  (void)ws_bytes;
+  if (n_pts < 0) return fail(FE_ERR_ARG, "fe_nuclear_fp64: n_pts < 0");
+  if (n_pts == 0) return FE_OK;
+  if (!d_table || !d_pts || !d_out) return fail(FE_ERR_ARG, "fe_nuclear_fp64: null argument");
+  fe_nuclear_kernel<<<(n_pts + 255) / 256, 256, 0, st>>>(static_cast<const unsigned char*>(d_table),
+                                                         d_pts, n_pts, d_out);
+  FE_CUDA(cudaGetLastError());
+  return FE_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Boys function kernel (tests and the boys() API)
+// ---------------------------------------------------------------------------
+template <int M>
+__global__ void fe_boys_kernel(const double* __restrict__ T, int n, double* __restrict__ F) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double f[M + 1];
+  fe_boys_f64<M>(T[i], f);
+#pragma unroll
+  for (int m = 0; m <= M; ++m) F[size_t(i) * (M + 1) + m] = f[m];
+}
+
+extern "C" int fe_boys_fp64(const double* d_T, int n, int mmax, double* d_F, cudaStream_t st) {
+  if (n < 0 || !d_T || !d_F) return fail(FE_ERR_ARG, "fe_boys_fp64: bad argument");
+  if (mmax < 0 || mmax > FE_MMAX) return fail(FE_ERR_UNSUPPORTED, "fe_boys_fp64: mmax %d outside 0..%d", mmax, FE_MMAX);
+  if (n == 0) return FE_OK;
+  const int blk = 128, grd = (n + blk - 1) / blk;
+  switch (mmax) {
+#define FE_B(m) case m: fe_boys_kernel<m><<<grd, blk, 0, st>>>(d_T, n, d_F); break;
+    FE_B(0) FE_B(1) FE_B(2) FE_B(3) FE_B(4) FE_B(5) FE_B(6) FE_B(7) FE_B(8) FE_B(9)
+#undef FE_B
+  }
+  FE_CUDA(cudaGetLastError());
+  return FE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// FMA throughput probe: the FP64 / FP32 pipe peak used as the roofline
+// denominator (8 independent FMA chains per thread, no memory traffic).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) fe_peak_kernel(long long iters, T* out) {
+  T a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = T(threadIdx.x + k) * T(1e-6);
+  const T b = T(0.9999999), c = T(1e-7);
+#pragma unroll 4
+  for (long long it = 0; it < iters; ++it)
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = fe_fma(a[k], b, c);
+  T s = T(0);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += a[k];
+  if (threadIdx.x == 0) out[blockIdx.x] = s;
+}
+
+extern "C" int fe_peak_run(int fp64, long long iters, int blocks, void* d_out, cudaStream_t st) {
+  if (iters <= 0 || blocks <= 0 || !d_out) return fail(FE_ERR_ARG, "fe_peak_run: bad argument");
+  if (fp64)
+    fe_peak_kernel<double><<<blocks, 256, 0, st>>>(iters, static_cast<double*>(d_out));
+  else
+    fe_peak_kernel<float><<<blocks, 256, 0, st>>>(iters, static_cast<float*>(d_out));
+  FE_CUDA(cudaGetLastError());
+  return FE_OK;
+}

@@ -1,0 +1,363 @@
+"""Generate ``classes_gen.cuh``: compile-time data and unrolled code per class L.
+
+    python fastesp_b200/csrc/gen_classes.py        (run by the build; output committed)
+
+For every angular class L = la + lb (0..8) this emits
+
+* the term count, FP64/FP32 record strides and Boys order;
+* ``fe_poly_L<L>``: s = sum_k G_k R^alpha_k F_m_k for NP points per thread in
+  nested Horner form -- per Boys order m the polynomial sum_k G_k R^alpha_k is
+  evaluated x-outer / y / z-inner with fused multiply-adds, every coefficient
+  is read once and reused for the NP points;
+* ``fe_grad_L<L>``: the same sum and its gradient with respect to R (adjoint);
+* the sparse contraction rows M0[k, t] (etab -> G) used by the table builder,
+  with t in the compact order of ``hermite.t_index``;
+* the Boys Taylor grid F_n(i h), n = 0..NTAB-1, computed here in 40-digit
+  arithmetic (mpmath), and the per-order asymptotic thresholds.
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parents[1]))
+
+from fastesp_b200 import hermite as H  # noqa: E402
+
+LMAX = 2 * H.LMAX_SHELL        # largest class
+MMAX = LMAX + 1                # largest Boys order needed (adjoint needs L+1)
+TAYLOR_K = 8                   # Taylor terms of the tabulated branch
+GRID_H = 1.0 / 16.0            # grid spacing of the tabulated branch
+GRID_TMAX = 12.0               # tabulated branch covers 0 <= T < GRID_TMAX
+NTAB = MMAX + TAYLOR_K         # orders stored per grid row
+VARS = ("x", "y", "z")
+
+
+# --------------------------------------------------------------------------
+# Horner emission
+# --------------------------------------------------------------------------
+class Emitter:
+    def __init__(self, real="Real"):
+        self.lines = []
+        self.nops = 0
+        self.real = real
+
+    def w(self, s):
+        self.lines.append("  " + s)
+
+    def horner(self, terms, depth, acc, coef):
+        """Emit acc[depth][j] = sum_terms coef(k) * v^e ... over VARS[depth:].
+
+        ``terms``: {exponent tuple over VARS[depth:]: k}.  ``coef(k)`` returns
+        (setup_line or None, scalar expression).
+        """
+        v = VARS[depth]
+        groups = {}
+        for e, k in terms.items():
+            groups.setdefault(e[0], {})[e[1:]] = k
+        emax = max(groups)
+        dst = acc[depth]
+        first = True
+        for e in range(emax, -1, -1):
+            if e in groups:
+                if depth == len(VARS) - 1:
+                    (k,) = groups[e].values()
+                    setup, sub = coef(k)
+                    if setup:
+                        self.w(setup)
+                    sub_j = sub
+                else:
+                    self.horner(groups[e], depth + 1, acc, coef)
+                    sub_j = f"{acc[depth + 1]}[j]"
+                if first:
+                    self.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) {dst}[j] = {sub_j};")
+                    first = False
+                else:
+                    self.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) "
+                           f"{dst}[j] = fe_fma({dst}[j], {v}[j], {sub_j});")
+                    self.nops += 1
+            elif not first:
+                self.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) {dst}[j] *= {v}[j];")
+                self.nops += 1
+
+
+def poly_m_major(L):
+    keys, _ = H.class_terms(L)
+    em = Emitter()
+    by_m = {}
+    for k, (ax, ay, az, m) in enumerate(keys):
+        by_m.setdefault(m, {})[(ax, ay, az)] = k
+    acc = ("ha", "hb", "hc")
+    first = True
+    for m in sorted(by_m):
+        def coef(k):
+            return f"const Real g{k} = g[{k}];", f"g{k}"
+        em.horner(by_m[m], 0, acc, coef)
+        if first:
+            em.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) s[j] = F[j][{m}] * ha[j];")
+            first = False
+        else:
+            em.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) s[j] = fe_fma(F[j][{m}], ha[j], s[j]);")
+        em.nops += 1
+    return em
+
+
+def poly_alpha_major(L):
+    keys, _ = H.class_terms(L)
+    em = Emitter()
+    by_a = {}
+    for k, (ax, ay, az, m) in enumerate(keys):
+        by_a.setdefault((ax, ay, az), []).append((k, m))
+    acc = ("ha", "hb", "hc")
+
+    def coef(a):
+        ks = by_a[a]
+        lines = []
+        k0, m0 = ks[0]
+        lines.append(f"const Real g{k0} = g[{k0}]; "
+                     f"FE_UNROLL for (int j = 0; j < NP; ++j) hd[j] = g{k0} * F[j][{m0}];")
+        em.nops += 1
+        for k, m in ks[1:]:
+            lines.append(f"const Real g{k} = g[{k}]; "
+                         f"FE_UNROLL for (int j = 0; j < NP; ++j) hd[j] = fe_fma(g{k}, F[j][{m}], hd[j]);")
+            em.nops += 1
+        return " ".join(lines), "hd[j]"
+
+    alpha_terms = {a: a for a in by_a}
+    em.horner(alpha_terms, 0, acc, coef)
+    em.w("FE_UNROLL for (int j = 0; j < NP; ++j) s[j] = ha[j];")
+    return em
+
+
+def poly_function(L):
+    a = poly_m_major(L)
+    b = poly_alpha_major(L)
+    em, tag = (a, "m-major") if a.nops <= b.nops else (b, "alpha-major")
+    out = [f"// class L={L}: {H.n_terms(L)} terms, {em.nops} fused ops per point ({tag})",
+           "template <typename Real, int NP>",
+           f"__device__ __forceinline__ void fe_poly_L{L}(const Real* __restrict__ g,",
+           "    const Real (&x)[NP], const Real (&y)[NP], const Real (&z)[NP],",
+           f"    const Real (&F)[NP][{L + 1}], Real (&s)[NP]) {{",
+           "  Real ha[NP], hb[NP], hc[NP], hd[NP];",
+           "  (void)hb; (void)hc; (void)hd;"]
+    out += em.lines
+    out.append("}")
+    return out, em.nops
+
+
+def grad_function(L):
+    """s = sum_k G_k R^a F_m and dS/dR_c = sum_k G_k (a_c R^(a-e_c) F_m - 2p R_c R^a F_(m+1)).
+
+    Written as s, u = sum_k G_k R^a F_(m+1) and the three partial derivatives
+    of the monomials, each again in Horner form over exponents; F carries
+    orders 0..L+1.
+    """
+    keys, _ = H.class_terms(L)
+    em = Emitter()
+    acc = ("ha", "hb", "hc")
+    outs = []
+    # value s and u: same monomials, Boys order m and m+1
+    for name, shift in (("s", 0), ("u", 1)):
+        by_m = {}
+        for k, (ax, ay, az, m) in enumerate(keys):
+            by_m.setdefault(m + shift, {})[(ax, ay, az)] = k
+        first = True
+        for m in sorted(by_m):
+            em.horner(by_m[m], 0, acc, lambda k: (f"const Real g{k}_{name}{m} = g[{k}];",
+                                                 f"g{k}_{name}{m}"))
+            op = (f"{name}[j] = F[j][{m}] * ha[j];" if first else
+                  f"{name}[j] = fe_fma(F[j][{m}], ha[j], {name}[j]);")
+            em.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) {op}")
+            first = False
+    # derivative of the monomials: d/dR_c R^a = a_c R^(a - e_c)
+    for c, cname in enumerate(("dx", "dy", "dz")):
+        by_m = {}
+        for k, key in enumerate(keys):
+            a = list(key[:3])
+            m = key[3]
+            if a[c] == 0:
+                continue
+            fac = a[c]
+            a[c] -= 1
+            by_m.setdefault(m, {})[tuple(a)] = (k, fac)
+        first = True
+        for m in sorted(by_m):
+            em.horner(by_m[m], 0, acc,
+                      lambda kf, c=c, m=m: (f"const Real g{kf[0]}_d{c}{m} = "
+                                            f"Real({kf[1]}) * g[{kf[0]}];",
+                                            f"g{kf[0]}_d{c}{m}"))
+            op = (f"{cname}[j] = F[j][{m}] * ha[j];" if first else
+                  f"{cname}[j] = fe_fma(F[j][{m}], ha[j], {cname}[j]);")
+            em.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) {op}")
+            first = False
+        if first:
+            em.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) {cname}[j] = Real(0);")
+    out = [f"// class L={L}: value, F_(m+1) companion sum and monomial derivatives",
+           "template <typename Real, int NP>",
+           f"__device__ __forceinline__ void fe_grad_L{L}(const Real* __restrict__ g,",
+           "    const Real (&x)[NP], const Real (&y)[NP], const Real (&z)[NP],",
+           f"    const Real (&F)[NP][{L + 2}], Real (&s)[NP], Real (&u)[NP],",
+           "    Real (&dx)[NP], Real (&dy)[NP], Real (&dz)[NP]) {",
+           "  Real ha[NP], hb[NP], hc[NP];",
+           "  (void)hb; (void)hc;"]
+    out += em.lines
+    out.append("}")
+    return out
+
+
+# --------------------------------------------------------------------------
+# Boys grid and thresholds (40-digit reference values)
+# --------------------------------------------------------------------------
+def boys_mp(m, T):
+    import mpmath as mp
+    if T == 0:
+        return mp.mpf(1) / (2 * m + 1)
+    a = mp.mpf(m) + mp.mpf(1) / 2
+    return mp.gammainc(a, 0, T) / (2 * mp.power(T, a))
+
+
+def boys_grid():
+    import mpmath as mp
+    mp.mp.dps = 40
+    nrow = int(round(GRID_TMAX / GRID_H)) + 2
+    rows = []
+    for i in range(nrow):
+        T = mp.mpf(i) * mp.mpf(GRID_H)
+        rows.append([float(boys_mp(n, T)) for n in range(NTAB)])
+    return rows
+
+
+def asym_thresholds(rel=1e-16):
+    """Smallest T (on a 0.25 grid) from which the asymptotic Boys vector
+    F_m = (2m-1)!!/2^(m+1) sqrt(pi/T^(2m+1)) is within ``rel`` of F_m for all
+    m <= M, for every M <= MMAX."""
+    import mpmath as mp
+    mp.mp.dps = 40
+    out = []
+    for M in range(MMAX + 1):
+        T = 120.0
+        while T > 1.0:
+            Tm = mp.mpf(T - 0.25)
+            ok = True
+            for m in range(M + 1):
+                ex = boys_mp(m, Tm)
+                df = mp.mpf(1)
+                for q in range(1, 2 * m, 2):
+                    df *= q
+                asy = df / mp.power(2, m + 1) * mp.sqrt(mp.pi / mp.power(Tm, 2 * m + 1))
+                if abs(asy - ex) / ex > rel:
+                    ok = False
+                    break
+            if not ok:
+                break
+            T -= 0.25
+        out.append(T)
+    return out
+
+
+def main() -> int:
+    out = ["// Generated by gen_classes.py -- do not edit.",
+           "#pragma once",
+           "#ifndef FE_UNROLL",
+           "#define FE_UNROLL _Pragma(\"unroll\")",
+           "#endif",
+           "",
+           f"#define FE_NCLASS {LMAX + 1}",
+           f"#define FE_MMAX {MMAX}",
+           f"#define FE_BOYS_NTAB {NTAB}",
+           f"#define FE_BOYS_TAYLOR_K {TAYLOR_K}",
+           f"#define FE_BOYS_GRID_INV_H {1.0 / GRID_H!r}",
+           f"#define FE_BOYS_GRID_H {GRID_H!r}",
+           f"#define FE_BOYS_GRID_TMAX {GRID_TMAX!r}",
+           ""]
+    nts = [H.n_terms(L) for L in range(LMAX + 1)]
+    out.append("static constexpr int fe_class_nterm[FE_NCLASS] = {"
+               + ", ".join(map(str, nts)) + "};")
+    out.append("static constexpr int fe_class_rec64[FE_NCLASS] = {"
+               + ", ".join(str(H.record_stride(L)) for L in range(LMAX + 1)) + "};")
+    out.append("static constexpr int fe_class_rec32[FE_NCLASS] = {"
+               + ", ".join(str(H.record_stride_f32(L)) for L in range(LMAX + 1)) + "};")
+    out.append("static constexpr int fe_class_ntri[FE_NCLASS] = {"
+               + ", ".join(str(len(H.t_index(L))) for L in range(LMAX + 1)) + "};")
+    out.append("")
+    ths = asym_thresholds()
+    out.append("// T above which the Boys vector F_0..F_M is its asymptotic form to 1e-16")
+    out.append("static constexpr double fe_boys_asym_T[FE_MMAX + 1] = {"
+               + ", ".join(repr(t) for t in ths) + "};")
+    out.append("")
+    # Boys grid
+    rows = boys_grid()
+    out.append(f"// F_n(i*h), i = 0..{len(rows) - 1}, n = 0..FE_BOYS_NTAB-1")
+    out.append(f"#define FE_BOYS_NROW {len(rows)}")
+    out.append("__device__ const double fe_boys_grid[FE_BOYS_NROW * FE_BOYS_NTAB] = {")
+    for r in rows:
+        out.append("  " + ", ".join(repr(v) for v in r) + ",")
+    out.append("};")
+    out.append("")
+    # contraction rows
+    for L in range(LMAX + 1):
+        keys, rows_ = H.class_terms(L)
+        tix = H.t_index(L)
+        ptr, col, val = [0], [], []
+        for r in rows_:
+            for t, c in r:
+                col.append(tix[t])
+                val.append(c)
+            ptr.append(len(col))
+        out.append(f"// class L={L}: M0 rows (etab compact index -> G term), nnz={len(col)}")
+        out.append(f"__constant__ short fe_m0_ptr_L{L}[{len(ptr)}] = {{" + ", ".join(map(str, ptr)) + "};")
+        out.append(f"__constant__ short fe_m0_col_L{L}[{len(col)}] = {{" + ", ".join(map(str, col)) + "};")
+        out.append(f"__constant__ signed char fe_m0_m_L{L}[{len(keys)}] = {{"
+                   + ", ".join(str(k[3]) for k in keys) + "};")
+        vals = ", ".join(repr(float(v)) for v in val)
+        out.append(f"__constant__ float fe_m0_val_L{L}[{len(val)}] = {{{vals}}};")
+        assert all(abs(v) < 2 ** 24 and float(int(v)) == v for v in val)
+    out.append("")
+    # polynomial evaluators
+    nops = []
+    for L in range(LMAX + 1):
+        lines, n = poly_function(L)
+        nops.append(n)
+        out += lines
+        out.append("")
+    out.append("static constexpr int fe_class_polyops[FE_NCLASS] = {"
+               + ", ".join(map(str, nops)) + "};")
+    out.append("")
+    for L in range(LMAX + 1):
+        out += grad_function(L)
+        out.append("")
+    # compile-time dispatch on the class
+    out.append("template <int L, typename Real, int NP>")
+    out.append("__device__ __forceinline__ void fe_poly(const Real* __restrict__ g,")
+    out.append("    const Real (&x)[NP], const Real (&y)[NP], const Real (&z)[NP],")
+    out.append("    const Real (&F)[NP][L + 1], Real (&s)[NP]) {")
+    for L in range(LMAX + 1):
+        kw = "if" if L == 0 else "else if"
+        out.append(f"  {kw} constexpr (L == {L}) fe_poly_L{L}<Real, NP>(g, x, y, z, F, s);")
+    out.append("}")
+    out.append("")
+    out.append("template <int L, typename Real, int NP>")
+    out.append("__device__ __forceinline__ void fe_grad(const Real* __restrict__ g,")
+    out.append("    const Real (&x)[NP], const Real (&y)[NP], const Real (&z)[NP],")
+    out.append("    const Real (&F)[NP][L + 2], Real (&s)[NP], Real (&u)[NP],")
+    out.append("    Real (&dx)[NP], Real (&dy)[NP], Real (&dz)[NP]) {")
+    for L in range(LMAX + 1):
+        kw = "if" if L == 0 else "else if"
+        out.append(f"  {kw} constexpr (L == {L}) fe_grad_L{L}<Real, NP>(g, x, y, z, F, s, u, dx, dy, dz);")
+    out.append("}")
+    out.append("")
+    out.append("__constant__ int fe_c_rec64[FE_NCLASS] = {"
+               + ", ".join(str(H.record_stride(L)) for L in range(LMAX + 1)) + "};")
+    out.append("__constant__ int fe_c_rec32[FE_NCLASS] = {"
+               + ", ".join(str(H.record_stride_f32(L)) for L in range(LMAX + 1)) + "};")
+    out.append("__constant__ int fe_c_nterm[FE_NCLASS] = {"
+               + ", ".join(map(str, nts)) + "};")
+    (HERE / "classes_gen.cuh").write_text("\n".join(out) + "\n")
+    print("classes_gen.cuh:", len(out), "lines; poly ops", nops, "terms", nts,
+          "asym T", ths)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

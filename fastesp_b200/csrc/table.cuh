@@ -1,0 +1,41 @@
+// Device pair-table layout, shared by the builder, the evaluators and the host.
+//
+// One caller-allocated buffer holds the whole table:
+//
+//   [FeTableHdr][pad to 256][class 0 FP64 records][class 1 ...]...[class 8]
+//                           [class 0 FP32 records]...[atoms: Z[n], xyz[3n]]
+//
+// Pairs are grouped by angular class L = la + lb.  A class-L FP64 record is
+// fe_class_rec64[L] doubles: [p, Px, Py, Pz, K, G_0 .. G_(nt-1), pad], so the
+// records of a tile are one contiguous, 16-byte-aligned run that a single
+// bulk copy moves into shared memory.  Within a class, pairs keep the order of
+// the reference builder: shell pairs (si <= sj) in shell order, then
+// primitive pairs with the primitive of shell si outer.
+//
+// FP32 records (mixed-precision evaluator) are fe_class_rec32[L] floats:
+// [p, Px_hi, Py_hi, Pz_hi, Px_lo, Py_lo, Pz_lo, K, G_0 ..] (pad to 16 bytes).
+#pragma once
+#include <cstdint>
+
+#define FE_NCLASS_MAX 16
+#define FE_TABLE_MAGIC 0x34364546   // "FE64"
+
+struct FeTableHdr {
+  int32_t magic;
+  int32_t nclass;
+  int32_t n_atoms;
+  int32_t rule;                      // screening rule used by the build
+  double tol;                        // screening threshold used by the build
+  int32_t count[FE_NCLASS_MAX];      // kept pairs per class (device-written)
+  int32_t cap[FE_NCLASS_MAX];        // record capacity per class
+  int64_t off64[FE_NCLASS_MAX];      // byte offset of the FP64 records of class L
+  int64_t off32[FE_NCLASS_MAX];      // byte offset of the FP32 records of class L
+  int64_t off_atoms;                 // byte offset of Z[n_atoms] then xyz[3 n_atoms]
+  int64_t bytes;                     // total bytes of the table buffer
+  double sum_rule;                   // Tr(P S) accumulated by the build
+  int32_t has32;                     // FP32 records are current
+  int32_t pad_[3];
+};
+
+static_assert(sizeof(FeTableHdr) <= 512, "header must fit its slot");
+#define FE_TABLE_HDR_BYTES 512

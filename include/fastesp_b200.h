@@ -1,0 +1,159 @@
+/* fastesp_b200 -- C ABI of the B200 exact-ESP library (libfastesp_b200.so).
+ *
+ * The reference (ZidongS/fastesp) reaches its native code through two
+ * executables and files: ``build_pairs basis.bin pairs.bin tol``
+ * (fastesp/native/build_pairs.cpp:162-425, called from fastesp/cli.py:143-150)
+ * and ``esp_gpu pairs.bin out.txt`` (fastesp/native/esp_gpu.cu:232-326, called
+ * from fastesp/cli.py:153-168).  This header replaces both with in-process
+ * calls.  The basis description is the reference's ``basis_payload`` dict
+ * (fastesp/table.py:268-293) field for field.
+ *
+ * Conventions
+ *  - Every device buffer is allocated by the caller; the library allocates no
+ *    device memory.  Sizes come from fe_plan_sizes / fe_eval_ws_bytes.
+ *  - Calls are stream-ordered and asynchronous unless stated otherwise.
+ *  - Every function returns FE_OK (0) or an FE_ERR_* code and never exits the
+ *    process; fe_last_error() gives the message of the calling thread's last
+ *    failure.  Kernels report anomalies (a bounded wait that gave up, a
+ *    capacity overflow) in a device status word read by fe_status().
+ */
+#ifndef FASTESP_B200_H
+#define FASTESP_B200_H
+
+#include <stddef.h>
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FE_OK 0
+#define FE_ERR_ARG 1          /* invalid argument or shape */
+#define FE_ERR_CUDA 2         /* a CUDA runtime call failed */
+#define FE_ERR_SIZE 3         /* a caller buffer is too small */
+#define FE_ERR_UNSUPPORTED 4  /* angular momentum above g, or similar */
+#define FE_ERR_DEVICE 5       /* the device status word reports a failure */
+
+#define FE_NCLASS 9           /* angular classes L = la + lb = 0..8 */
+
+#define FE_RULE_NUMPY 0       /* keep unless K*bound/max(dmin, 0.05) < tol (fastesp/table.py:193) */
+#define FE_RULE_NATIVE 1      /* drop if K*bound/max(dmin - reff, 0.05) < tol (build_pairs.cpp:326-328) */
+
+/* Host copy of the basis payload (fastesp/table.py:268-293): per Cartesian
+ * function its atom, primitive count and offset, Cartesian exponents, shell
+ * id and centre; per primitive exponent and coefficient; per atom Z and xyz. */
+typedef struct fe_basis {
+  int n_func, n_prim, n_atoms;
+  const int *fn_atom, *fn_nprim, *fn_off, *fn_lx, *fn_ly, *fn_lz, *fn_shell;
+  const double *fc;      /* (n_func, 3) */
+  const double *pexp;    /* (n_prim,)  */
+  const double *pcoef;   /* (n_prim,)  */
+  const double *Z;       /* (n_atoms,) */
+  const double *xyz;     /* (n_atoms, 3) */
+} fe_basis;
+
+typedef struct fe_plan fe_plan;    /* opaque, host memory */
+
+typedef struct fe_sizes {
+  size_t plan_bytes;       /* device bytes of the uploaded plan */
+  size_t table_bytes;      /* device bytes of one pair table */
+  size_t build_ws_bytes;   /* device workspace of fe_table_build */
+  int n_shell, n_shell_pair, n_work;
+  int cap[FE_NCLASS];      /* primitive-pair slots per class (upper bound of kept pairs) */
+} fe_sizes;
+
+typedef struct fe_table_info {
+  int count[FE_NCLASS];    /* kept primitive pairs per class */
+  int n_pairs;             /* sum of count */
+  int n_atoms;
+  double sum_rule;         /* Tr(P S) = sum over pairs K (pi/p)^1.5 etab_0 (build_pairs.cpp:294-296) */
+  double tol;
+  int rule;
+  int has_f32;
+} fe_table_info;
+
+/* Version as major*10000 + minor*100 + patch. */
+int fe_version(void);
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char* fe_last_error(void);
+
+/* Read the device status word of the current device (synchronises the
+ * device); clear it when ``clear`` is non-zero.  Bits: 1 a bounded wait gave
+ * up, 2 an invalid class, 4 a capacity overflow. */
+int fe_status(unsigned* bits, int clear);
+
+/* Group the functions into shells (contiguous runs of fn_shell, as
+ * build_pairs.cpp:170-182 does), enumerate the shell pairs si <= sj and their
+ * primitive pairs in the reference's order, and size everything.
+ * Replaces the set-up half of build_pairs' main (build_pairs.cpp:162-187). */
+int fe_plan_create(const fe_basis* basis, fe_plan** out);
+void fe_plan_destroy(fe_plan* plan);
+int fe_plan_sizes(const fe_plan* plan, fe_sizes* sizes);
+
+/* Copy the plan to the caller's device buffer (plan_bytes, 256-byte aligned). */
+int fe_plan_upload(const fe_plan* plan, void* d_plan, cudaStream_t stream);
+
+/* Build the pair table on the GPU: E-coefficients, density-weighted Hermite
+ * table, G[alpha, m] contraction, screening bound and point screen, then an
+ * order-preserving compaction per class.  ``d_dens`` is the (n_func, n_func)
+ * Cartesian density, ``d_pts`` the (n_pts, 3) points (Bohr) used for the
+ * screen, ``rule`` FE_RULE_NUMPY or FE_RULE_NATIVE.  Replaces the hot loop and
+ * output of build_pairs (build_pairs.cpp:194-421) and build_table
+ * (fastesp/table.py:176-259). */
+int fe_table_build(const fe_plan* plan, const void* d_plan, const double* d_dens,
+                   const double* d_pts, int n_pts, double tol, int rule,
+                   void* d_table, void* d_ws, size_t ws_bytes, cudaStream_t stream);
+
+/* Bytes of a table whose class L holds up to cap[L] pairs (0 on bad input),
+ * and the byte offsets of its FP64 records, FP32 records and atom block. */
+size_t fe_table_bytes(const int* cap, int n_atoms);
+int fe_table_offsets(const int* cap, int n_atoms, size_t* off64, size_t* off32,
+                     size_t* off_atoms);
+
+/* Write the header and atom block of a table holding count[L] pairs per class
+ * whose FP64 records the caller copies in itself (import of a pairs.bin
+ * table, fastesp/table.py:143-170).  Synchronises ``stream``. */
+int fe_table_init(void* d_table, const int* count, int n_atoms, const double* Z,
+                  const double* xyz, cudaStream_t stream);
+
+/* (Re)derive the FP32 records of the mixed-precision path from the FP64 ones. */
+int fe_table_make_f32(void* d_table, cudaStream_t stream);
+
+/* Copy the table header to the host (synchronises ``stream``). */
+int fe_table_info_get(const void* d_table, fe_table_info* info, cudaStream_t stream);
+
+/* Workspace bytes of an evaluation of n_pts points (mode 0 FP64, 1 mixed). */
+size_t fe_eval_ws_bytes(int n_pts, int mode);
+
+/* V(C) = sum_A Z_A/|C-R_A| - sum_pairs K sum_k G_k R^alpha F_m(p R^2), all FP64,
+ * for the (n_pts, 3) points ``d_pts`` into ``d_out`` (n_pts,).  Replaces
+ * esp_pairs_kernel + esp_reduce_kernel (fastesp/native/esp_gpu.cu:161-229)
+ * and PairTable.esp (fastesp/table.py:102-104). */
+int fe_esp_fp64(const void* d_table, const double* d_pts, int n_pts, double* d_out,
+                void* d_ws, size_t ws_bytes, cudaStream_t stream);
+
+/* The electron part alone, int rho(r)/|r-C| dr (fastesp/table.py:73-93), FP64. */
+int fe_electron_fp64(const void* d_table, const double* d_pts, int n_pts, double* d_out,
+                     void* d_ws, size_t ws_bytes, cudaStream_t stream);
+
+/* The nuclear part alone, sum_A Z_A/|C-R_A| (fastesp/table.py:95-100); the
+ * workspace arguments are unused and may be null. */
+int fe_nuclear_fp64(const void* d_table, const double* d_pts, int n_pts, double* d_out,
+                    void* d_ws, size_t ws_bytes, cudaStream_t stream);
+
+/* Boys function F_0..F_mmax(T) for n arguments into d_F (n, mmax+1), FP64.
+ * Same values as fastesp.ints.boys (fastesp/ints.py:35-40). */
+int fe_boys_fp64(const double* d_T, int n, int mmax, double* d_F, cudaStream_t stream);
+
+/* FMA throughput probe (no counterpart in the reference): ``blocks`` blocks of
+ * 256 threads each run ``iters`` iterations of 8 independent FMA chains in FP64
+ * (fp64 != 0) or FP32, writing one value per block to d_out.  Timed by the
+ * caller; FLOPs = 16 * iters * 256 * blocks.  Used as the FP64/FP32 roofline. */
+int fe_peak_run(int fp64, long long iters, int blocks, void* d_out, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FASTESP_B200_H */

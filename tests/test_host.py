@@ -1,0 +1,152 @@
+"""Host-side pieces: MOLDEN reader, basis/density, Hermite tables, C ABI loading, planning."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from fastesp_b200 import Basis, basis_payload, cart_order, overlap_matrix, read_molden
+from fastesp_b200 import _lib, hermite as H, synth
+from fastesp_b200.basis import cartesian_overlap_block, pure_to_cartesian
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def test_spherical_transform_is_orthonormal():
+    """T S T^T = 1 for l <= 4 (reference tests/test_pipeline.py:82-86)."""
+    for l in range(5):
+        T = pure_to_cartesian(l)
+        S = cartesian_overlap_block(l)
+        assert np.abs(T @ S @ T.T - np.eye(2 * l + 1)).max() < 1e-14
+
+
+@pytest.mark.parametrize("tag", ["small", "tz6"])
+def test_density_and_overlap_match_reference(tag, request):
+    wfn, basis, P, g = request.getfixturevalue(f"{tag}_system")
+    np.testing.assert_allclose(P, g["density"], rtol=0, atol=1e-13 * np.abs(g["density"]).max())
+    S = overlap_matrix(basis)
+    np.testing.assert_allclose(S, g["overlap"], rtol=0, atol=1e-13)
+    # Tr(P S) = N_elec (reference tests/test_pipeline.py:102-111)
+    assert float((P * S).sum()) == pytest.approx(float(g["nelec"]), abs=1e-8)
+
+
+def test_mos_orthonormal_in_basis_metric():
+    sysm = synth.make_system("small", 3)
+    b = Basis(sysm.wavefunction())
+    t = b.block_transform()
+    s = t.T @ overlap_matrix(b) @ t
+    c = sysm.mo_coeff
+    assert np.abs(c.T @ s @ c - np.eye(c.shape[1])).max() < 1e-9
+
+
+def test_hermite_tables_match_reference(golden):
+    g = golden("pair_types")
+    np.testing.assert_array_equal(H.a_table(8), g["a8"])
+    for L in range(9):
+        keys, rows = H.class_terms(L)
+        T = L + 1
+        M0 = np.zeros((len(keys), T ** 3))
+        for k, row in enumerate(rows):
+            for (tx, ty, tz), c in row:
+                M0[k, (tx * T + ty) * T + tz] = c
+        np.testing.assert_array_equal(M0, g[f"M0_{L}"])
+        np.testing.assert_array_equal(np.array([k[:3] for k in keys]), g[f"mono_{L}"])
+
+
+def test_reader_parses_flags_and_counts(small_system):
+    wfn, basis, P, g = small_system
+    assert wfn.spherical[2] and wfn.spherical[3]
+    assert wfn.nelec == pytest.approx(float(g["nelec"]))
+    assert basis.n == sum(len(cart_order(sh.l)) for sh in wfn.shells)
+
+
+def _header_functions():
+    txt = (ROOT / "include" / "fastesp_b200.h").read_text()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(fe_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_loads_and_exports_header_symbols():
+    lib = _lib.lib()
+    names = _header_functions()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) <= set(_lib.exported_symbols())
+    assert lib.fe_version() >= 100
+
+
+def test_plan_sizes_without_gpu():
+    wfn, basis, P, pts = synth.load_workload("small", 50, seed=1)
+    pl = basis_payload(wfn, basis, P, pts)
+    keep = {k: np.ascontiguousarray(pl[k], np.int32)
+            for k in ("fn_atom", "fn_nprim", "fn_off", "fn_lx", "fn_ly", "fn_lz", "fn_shell")}
+    keep.update({k: np.ascontiguousarray(pl[k], np.float64) for k in ("fc", "pexp", "pcoef", "Z", "xyz")})
+    b = _lib.FeBasis(pl["n_func"], pl["n_prim"], pl["n_atoms"],
+                     *(keep[k].ctypes.data for k in ("fn_atom", "fn_nprim", "fn_off", "fn_lx", "fn_ly",
+                                                     "fn_lz", "fn_shell", "fc", "pexp", "pcoef", "Z", "xyz")))
+    h = C.c_void_p()
+    _lib.check(_lib.lib().fe_plan_create(C.byref(b), C.byref(h)))
+    s = _lib.FeSizes()
+    _lib.check(_lib.lib().fe_plan_sizes(h, C.byref(s)))
+    ns = len(wfn.shells)
+    assert s.n_shell == ns and s.n_shell_pair == ns * (ns + 1) // 2
+    nprim = [len(sh.exps) for sh in wfn.shells]
+    tot = sum(nprim[i] * nprim[j] for i in range(ns) for j in range(i, ns))
+    assert s.n_work == tot == sum(s.cap)
+    _lib.lib().fe_plan_destroy(h)
+
+
+def test_plan_rejects_bad_basis():
+    wfn, basis, P, pts = synth.load_workload("small", 10, seed=1)
+    pl = basis_payload(wfn, basis, P, pts)
+    pl["fn_shell"] = np.arange(basis.n, dtype=np.int32)      # every function its own shell
+    keep = {k: np.ascontiguousarray(pl[k], np.int32)
+            for k in ("fn_atom", "fn_nprim", "fn_off", "fn_lx", "fn_ly", "fn_lz", "fn_shell")}
+    keep.update({k: np.ascontiguousarray(pl[k], np.float64) for k in ("fc", "pexp", "pcoef", "Z", "xyz")})
+    b = _lib.FeBasis(pl["n_func"], pl["n_prim"], pl["n_atoms"],
+                     *(keep[k].ctypes.data for k in ("fn_atom", "fn_nprim", "fn_off", "fn_lx", "fn_ly",
+                                                     "fn_lz", "fn_shell", "fc", "pexp", "pcoef", "Z", "xyz")))
+    h = C.c_void_p()
+    rc = _lib.lib().fe_plan_create(C.byref(b), C.byref(h))
+    assert rc == 1
+    assert b"functions" in _lib.lib().fe_last_error()
+
+
+def test_table_layout_is_aligned():
+    cap = (C.c_int * 9)(*[7, 0, 3, 1, 0, 0, 2, 0, 0])
+    o64 = (C.c_size_t * 9)()
+    o32 = (C.c_size_t * 9)()
+    oa = C.c_size_t()
+    _lib.check(_lib.lib().fe_table_offsets(cap, 5, o64, o32, C.byref(oa)))
+    assert all(v % 256 == 0 for v in list(o64) + list(o32) + [oa.value])
+    assert _lib.lib().fe_table_bytes(cap, 5) >= oa.value + 5 * 32
+
+
+def test_basis_payload_file(tmp_path, small_system):
+    from fastesp_b200 import write_basis_payload
+    wfn, basis, P, g = small_system
+    pl = basis_payload(wfn, basis, P, g["points"])
+    write_basis_payload(tmp_path / "basis.bin", pl)
+    raw = (tmp_path / "basis.bin").read_bytes()
+    n = pl["n_func"]
+    expect = 32 + 7 * 4 * n + 8 * (3 * n + 2 * pl["n_prim"] + n * n + 3 * len(g["points"])
+                                  + 4 * pl["n_atoms"])
+    assert len(raw) == expect
+
+
+def test_synthetic_workload_shapes():
+    s = synth.make_system("frag54", 0)
+    b = Basis(s.wavefunction())
+    assert len(s.symbols) == 54 and sorted(set(s.symbols)) == ["C", "H", "N", "O"]
+    assert 1550 <= b.n <= 1750
+    assert 1950 <= sum(len(e) for e in b.exps) <= 2200
+    assert max(sh.l for sh in s.shells) == 3
+    pts = synth.vdw_surface_points(s.symbols, s.coords, 500, seed=2)
+    rad = np.array([1.4 * synth.BONDI[x] / 0.529177210903 for x in s.symbols])
+    d = np.linalg.norm(pts[:, None, :] - s.coords[None], axis=2)
+    assert (d >= rad[None, :] - 1e-9).all()
+    assert np.isclose(d / rad[None, :], 1.0, atol=1e-9).any(axis=1).all()
