@@ -141,7 +141,7 @@ def run_ours(args):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    wfn, basis, P, _ = synth.load_workload("frag54", 10, seed=1)
+    wfn, basis, P, _ = synth.load_workload("frag54", 10, seed=0)
     pts = synth.vdw_surface_points(wfn.symbols, wfn.coords, args.points, seed=1 + rank)
     dev = torch.device("cuda", local)
     P_d = torch.as_tensor(P, device=dev)
@@ -158,7 +158,7 @@ def run_ours(args):
     counts = tab.counts
     prec = args.precision
     tb = []
-    for i in range(args.warmup + max(3, args.steps // 2)):
+    for i in range(0 if args.eval_only else args.warmup + max(3, args.steps // 2)):
         flush.zero_()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
@@ -168,23 +168,29 @@ def run_ours(args):
         if i >= args.warmup:
             tb.append(a.elapsed_time(b))
         del t2
-    build_ms = statistics.median(tb)
+    build_ms = statistics.median(tb) if tb else None
 
-    # value: evaluation with the table resident
+    # value: evaluation with the table resident, both precisions
     out = torch.empty(args.points, dtype=torch.float64, device=dev)
     L = _lib.lib()
-    ws = torch.empty(max(256, L.fe_eval_ws_bytes(args.points, 0)), dtype=torch.uint8, device=dev)
+    ws = torch.empty(max(256, L.fe_eval_ws_bytes(args.points, 0), L.fe_eval_ws_bytes(args.points, 1)),
+                     dtype=torch.uint8, device=dev)
+    n64 = torch.zeros(1, dtype=torch.int64, device=dev)
 
-    def step():
+    def step_fp64():
         _lib.check(L.fe_esp_fp64(_lib.ptr(tab._buf), _lib.ptr(pts_d), args.points, _lib.ptr(out),
                                  _lib.ptr(ws), ws.numel(), _lib.stream_ptr()))
 
-    for _ in range(args.warmup):
-        flush.zero_()
-        step()
-    barrier()
-    times = []
-    with ClockSampler(local) as clk:
+    def step_mixed():
+        _lib.check(L.fe_esp_mixed(_lib.ptr(tab._buf), _lib.ptr(pts_d), args.points, _lib.ptr(out),
+                                  _lib.ptr(ws), ws.numel(), 0.0, None, _lib.stream_ptr()))
+
+    def timed(step, clk=None):
+        for _ in range(args.warmup):
+            flush.zero_()
+            step()
+        barrier()
+        times = []
         for _ in range(args.steps):
             flush.zero_()            # L2 flush between timed steps (not timed)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -194,14 +200,40 @@ def run_ours(args):
             b.synchronize()
             times.append(a.elapsed_time(b))
         barrier()
-    t_ms = sum(times)
-    t_ms_max = t_ms
-    if world > 1:
-        t = torch.tensor([t_ms, build_ms], device=dev)
+        t = sum(times)
+        if world > 1:
+            tt = torch.tensor([t], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt[0])
+        return t / args.steps
+
+    main_step, other_step = (step_mixed, step_fp64) if prec == "mixed" else (step_fp64, step_mixed)
+    with ClockSampler(local) as clk:
+        ms_per_step = timed(main_step)
+    ms_other = timed(other_step)
+    ms_fp64, ms_mixed = (ms_other, ms_per_step) if prec == "mixed" else (ms_per_step, ms_other)
+    if args.eval_only:
+        if rank == 0:
+            print(json.dumps({"eval_only": True, "mixed_ms": ms_mixed, "fp64_ms": ms_fp64,
+                              "points": args.points, "pairs": int(sum(counts))}))
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    if world > 1 and build_ms is not None:
+        t = torch.tensor([build_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms_max, build_ms = float(t[0]), float(t[1])
-    ms_per_step = t_ms_max / args.steps
+        build_ms = float(t[0])
     value = world * args.points / (ms_per_step * 1e-3)
+    # accuracy of the mixed path against the FP64 path on this run's points
+    step_fp64()
+    v64 = out.clone()
+    _lib.check(L.fe_esp_mixed(_lib.ptr(tab._buf), _lib.ptr(pts_d), args.points, _lib.ptr(out),
+                              _lib.ptr(ws), ws.numel(), 0.0, _lib.ptr(n64), _lib.stream_ptr()))
+    dv = (out - v64).abs()
+    mixed_err = {"max_abs": float(dv.max()), "rms": float(dv.pow(2).mean().sqrt()),
+                 "fp64_routed_pair_warp_evals": int(n64.item()),
+                 # warps of 32 threads x 4 points each evaluate every pair
+                 "pair_warp_evals": int(sum(counts)) * (((args.points + 511) // 512) * 4)}
 
     # e2e through the public API from pinned host buffers
     P_h = torch.as_tensor(P).pin_memory()
@@ -210,7 +242,7 @@ def run_ours(args):
 
     def e2e_step():
         t = build_table(wfn, basis, P_h, pts_h, tol=1e-12)
-        v = t.esp(pts_h.to(dev, non_blocking=True))
+        v = t.esp(pts_h.to(dev, non_blocking=True), precision=prec)
         res_h.copy_(v, non_blocking=True)
 
     for _ in range(max(1, args.warmup)):
@@ -242,14 +274,16 @@ def run_ours(args):
     parity = float(np.abs(gt.esp() - g["esp_t12"]).max())
     status = _lib.status(clear=True)
 
-    peak = peak_flops(torch, fp64=(prec == "fp64"))
+    peak64 = peak_flops(torch, fp64=True)
+    peak32 = peak_flops(torch, fp64=False)
     flops = algorithmic_flops(counts, args.points)
     achieved = flops / (ms_per_step * 1e-3)
+    peak = peak32 if prec == "mixed" else peak64
     traffic = None
-    prof = ROOT / "profiles" / "eval_f64_frag54_30000.json"
+    prof = ROOT / "profiles" / f"eval_{'mixed' if prec == 'mixed' else 'f64'}_frag54_30000.json"
     if prof.exists():
         traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
-    nsplit_launches = 2 if L.fe_eval_ws_bytes(args.points, 0) > 256 else 1
+    launches = 2 if L.fe_eval_ws_bytes(args.points, 1 if prec == "mixed" else 0) > 256 else 1
     line = {
         "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -259,14 +293,20 @@ def run_ours(args):
                    "pairs": int(sum(counts)), "pairs_per_class": counts,
                    "precision": prec, "l2": "flushed (256 MiB write) between timed steps",
                    "parallelism": f"points sharded across {world} GPU(s), table per GPU"},
+        "fp64_points_per_s": world * args.points / (ms_fp64 * 1e-3),
+        "mixed_points_per_s": world * args.points / (ms_mixed * 1e-3),
+        "mixed_over_fp64": ms_fp64 / ms_mixed,
+        "mixed_error_vs_fp64": mixed_err,
         "table_build_ms": build_ms,
         "e2e": e2e,
-        "roofline": {"bound": "fp64" if prec == "fp64" else "fp32", "achieved": achieved / 1e12,
-                     "peak": peak / 1e12, "unit": "TFLOP/s", "frac": achieved / peak,
-                     "traffic": traffic,
+        "roofline": {"bound": "fp32" if prec == "mixed" else "fp64",
+                     "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": traffic,
                      "peak_source": "measured FMA throughput (fe_peak_run) on this GPU, this run",
-                     "flops_per_step": flops},
-        "gpu_launches": args.steps * nsplit_launches,
+                     "flops_per_step": flops,
+                     "fp64_path": {"achieved": flops / (ms_fp64 * 1e-3) / 1e12,
+                                   "peak": peak64 / 1e12, "frac": flops / (ms_fp64 * 1e-3) / peak64}},
+        "gpu_launches": args.steps * launches,
         "parity_frag54_300_max_abs": parity,
         "device_status": status,
         "published_reference": PUBLISHED,
@@ -341,7 +381,7 @@ def run_reference(args):
     if rank != 0:
         return
     from fastesp_b200 import synth
-    wfn, basis, P, _ = synth.load_workload("frag54", 10, seed=1)
+    wfn, basis, P, _ = synth.load_workload("frag54", 10, seed=0)
     pts = synth.vdw_surface_points(wfn.symbols, wfn.coords, args.points, seed=1)
     per_step = []
     base = None
@@ -370,10 +410,12 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--points", type=int, default=30000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--eval-only", action="store_true",
+                    help="time only the two evaluators (short run for profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -56,3 +56,41 @@ FE_DEV void fe_boys_f64(const double T, double (&F)[M + 1]) {
     for (int m = M; m > 0; --m) F[m - 1] = fma(t2, F[m], e) * (1.0 / double(2 * m - 1));
   }
 }
+
+// FP32 Boys vector for the mixed-precision evaluator.  Asymptotic above
+// fe_boys32_asym_T[M] (2e-8 relative); below it a 6-term Taylor expansion
+// about the nearest point of a 1/4 grid over 0 <= T < 32 held in shared
+// memory (``grid``, truncation below 6e-9 relative), then the downward
+// recursion.  The FP32 thresholds of orders <= 6 lie below 32, so the common
+// classes have only these two branches; for higher orders the stretch from 32
+// to the threshold uses the upward recursion from erf.  ``rt`` is T^-1/2,
+// which the caller already has.
+template <int M>
+FE_DEV void fe_boys_f32(const float T, const float rt, const float* __restrict__ grid,
+                        float (&F)[M + 1]) {
+  constexpr float t_asym = fe_boys32_asym_T[M];
+  if (T >= t_asym) {
+    const float h = 0.5f * rt * rt;
+    F[0] = float(FE_SQRT_PI_2) * rt;
+#pragma unroll
+    for (int m = 0; m < M; ++m) F[m + 1] = F[m] * (float(2 * m + 1) * h);
+  } else if (t_asym > FE_BOYS32_GRID_TMAX && T >= FE_BOYS32_GRID_TMAX) {
+    const float h = 0.5f * rt * rt;
+    const float e = __expf(-T);
+    F[0] = float(FE_SQRT_PI_2) * rt * erff(T * rt);
+#pragma unroll
+    for (int m = 0; m < M; ++m) F[m + 1] = fmaf(float(2 * m + 1), F[m], -e) * h;
+  } else {
+    const int i = __float2int_rn(T * FE_BOYS32_GRID_INV_H);
+    const float d = -(T - float(i) * FE_BOYS32_GRID_H);
+    const float* row = grid + i * FE_BOYS32_NTAB + M;
+    float f = row[FE_BOYS32_TAYLOR_K - 1];
+#pragma unroll
+    for (int k = FE_BOYS32_TAYLOR_K - 2; k >= 0; --k) f = fmaf(f, d * (1.0f / float(k + 1)), row[k]);
+    F[M] = f;
+    const float e = __expf(-T);
+    const float t2 = T + T;
+#pragma unroll
+    for (int m = M; m > 0; --m) F[m - 1] = fmaf(t2, F[m], e) * (1.0f / float(2 * m - 1));
+  }
+}

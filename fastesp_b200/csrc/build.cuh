@@ -240,7 +240,7 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
     for (int q = rp[k]; q < rp[k + 1]; ++q) s += double(rv[q]) * etab[rc[q]];
     const double g = cf * pw[rm[k]] * s;
     anyg |= (g != 0.0);
-    rec[5 + k] = g;
+    rec[6 + k] = g;
   }
   if (a.rule == 1 && !anyg) return;
 
@@ -281,8 +281,9 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
   rec[2] = P[1];
   rec[3] = P[2];
   rec[4] = K;
+  rec[5] = __dmul_rn(K, bound);
 #pragma unroll
-  for (int k = 5 + NT; k < REC; ++k) rec[k] = 0.0;
+  for (int k = 6 + NT; k < REC; ++k) rec[k] = 0.0;
   a.keep[slot] = 1;
 }
 
@@ -406,7 +407,8 @@ __global__ void __launch_bounds__(FE_SCAN_BLOCK) fe_scan_apply_kernel(
   if (i < n) pos[i] = bsum[blockIdx.x] + buf[threadIdx.x] - v;
 }
 
-// FP32 records of the mixed-precision path from the FP64 records.
+// Mixed-precision records from the FP64 records: every FP64 value as a float
+// hi/lo pair (layout in table.cuh).
 __global__ void fe_make_f32_kernel(unsigned char* table) {
   FeTableHdr* hdr = reinterpret_cast<FeTableHdr*>(table);
   const int L = blockIdx.y;
@@ -414,19 +416,21 @@ __global__ void fe_make_f32_kernel(unsigned char* table) {
   const int R64 = fe_c_rec64[L], R32 = fe_c_rec32[L], NT = fe_c_nterm[L];
   const double* src = reinterpret_cast<const double*>(table + hdr->off64[L]);
   float* dst = reinterpret_cast<float*>(table + hdr->off32[L]);
+  auto split = [](double v, float& hi, float& lo) {
+    hi = float(v);
+    lo = float(v - double(hi));
+  };
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double* r = src + size_t(i) * R64;
     float* o = dst + size_t(i) * R32;
-    o[0] = float(r[0]);
+    split(r[0], o[0], o[1]);
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const float hi = float(r[1 + k]);
-      o[1 + k] = hi;
-      o[4 + k] = float(r[1 + k] - double(hi));
-    }
-    o[7] = float(r[4]);
-    for (int k = 0; k < NT; ++k) o[8 + k] = float(r[5 + k]);
-    for (int k = 8 + NT; k < R32; ++k) o[k] = 0.0f;
+    for (int k = 0; k < 3; ++k) split(r[1 + k], o[2 + k], o[5 + k]);
+    split(r[4], o[8], o[9]);
+    o[10] = float(r[5]);                 // K * bound (+inf when unknown)
+    o[11] = float(1.0 / sqrt(r[0]));     // p^-1/2
+    for (int k = 0; k < NT; ++k) split(r[6 + k], o[12 + k], o[12 + NT + k]);
+    for (int k = 12 + 2 * NT; k < R32; ++k) o[k] = 0.0f;
   }
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) hdr->has32 = 1;
 }

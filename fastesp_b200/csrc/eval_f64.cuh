@@ -13,9 +13,9 @@
 // multiply-adds.  Per point, per pair: R = C - P, T = p|R|^2, the Boys vector
 // F_0..F_L, and the class polynomial in nested Horner form.
 //
-// nsplit == 1: the epilogue adds the nuclear term and writes V directly.
-// nsplit > 1 : each split writes its partial electron sum; fe_reduce_kernel
-// adds the splits in a fixed order (deterministic) and the nuclear term.
+// Every (point block, split) writes its partial electron sums to its own row of
+// the workspace; fe_reduce_kernel adds all rows in a fixed order
+// (deterministic) and the nuclear term.
 #pragma once
 #include "boys.cuh"
 #include "table.cuh"
@@ -32,10 +32,8 @@ struct FeEvalArgs {
   const double* pts;               // (npts, 3) Bohr
   int npts;
   int nsplit;
-  double* partial;                 // [nsplit][ld] when nsplit > 1
+  double* partial;                 // [nsplit][ld] partial electron sums of this kernel
   int ld;
-  double* out;                     // (npts,) when nsplit == 1
-  int mode;                        // 0: V = nuclear - electron, 1: electron only
 };
 
 // Pairs of class L per stage / tile.
@@ -49,37 +47,98 @@ __constant__ int fe_c_tile64[FE_NCLASS] = {
   FE_STAGE_BYTES / (8 * fe_class_rec64[6]), FE_STAGE_BYTES / (8 * fe_class_rec64[7]),
   FE_STAGE_BYTES / (8 * fe_class_rec64[8])};
 
-// The block's share of class L: pairs [lo, hi).
+// The block's share of every class, kept in shared memory: pairs [lo, hi) of
+// class L, cut into ntile tiles; ``total`` tiles in all.
 struct FeBlockWork {
   int lo[FE_NCLASS];
+  int hi[FE_NCLASS];
   int ntile[FE_NCLASS];
   int total;
 };
 
-FE_DEV void fe_block_work(const FeTableHdr* hdr, int split, int nsplit,
-                          const int* tile_sz, FeBlockWork& w) {
-  w.total = 0;
-#pragma unroll
+// Thread 0 only.  Classes outside [llo, lhi] get no tiles.
+FE_DEV void fe_block_work(const FeTableHdr* hdr, int split, int nsplit, const int* tile_sz,
+                          int llo, int lhi, FeBlockWork& w) {
+  int total = 0;
   for (int L = 0; L < FE_NCLASS; ++L) {
-    const long long n = hdr->count[L];
-    const int lo = int(n * split / nsplit);
-    const int hi = int(n * (split + 1) / nsplit);
-    w.lo[L] = lo;
-    w.ntile[L] = (hi - lo + tile_sz[L] - 1) / tile_sz[L];
-    w.total += w.ntile[L];
+    const long long n = (L >= llo && L <= lhi) ? hdr->count[L] : 0;
+    w.lo[L] = int(n * split / nsplit);
+    w.hi[L] = int(n * (split + 1) / nsplit);
+    w.ntile[L] = (w.hi[L] - w.lo[L] + tile_sz[L] - 1) / tile_sz[L];
+    total += w.ntile[L];
   }
+  w.total = total;
 }
 
-// Item i of the block -> (class, first pair, pair count).
-FE_DEV void fe_item(const FeTableHdr* hdr, const FeBlockWork& w, int split, int nsplit,
-                    const int* tile_sz, int i, int& L, int& first, int& n) {
+// Tile i of the block -> (class, first pair, pair count).
+FE_DEV void fe_item(const FeBlockWork& w, const int* tile_sz, int i, int& L, int& first, int& n) {
   L = 0;
   while (L < FE_NCLASS - 1 && i >= w.ntile[L]) { i -= w.ntile[L]; ++L; }
-  const long long cnt = hdr->count[L];
-  const int hi = int(cnt * (split + 1) / nsplit);
   first = w.lo[L] + i * tile_sz[L];
-  n = min(tile_sz[L], hi - first);
+  n = min(tile_sz[L], w.hi[L] - first);
 }
+
+// The block's tiles of records stream through a FE_NSTAGE ring of shared-memory
+// stages: thread 0 issues 1-D TMA bulk copies that complete on per-stage
+// mbarriers; every thread waits for the current stage, evaluates it, and the
+// block releases it (a barrier) before thread 0 refills it.  ``elem`` bytes per
+// record word, class record words ``rec[L]``, class byte offsets ``off[L]``.
+struct FeTilePipe {
+  const unsigned char* table;
+  const int* tile_sz;
+  const int* rec;
+  const int64_t* off;
+  int elem;
+  unsigned char* smem;
+  uint64_t* bar;
+  FeBlockWork* w;
+  // optional second record array of the same pairs, staged right after the
+  // first one's n records (rec2 == nullptr: none)
+  const int* rec2 = nullptr;
+  const int64_t* off2 = nullptr;
+  int elem2 = 0;
+
+  FE_DEV void start(const FeTableHdr* hdr, int split, int nsplit, int llo, int lhi) {
+    if (threadIdx.x == 0) {
+      fe_block_work(hdr, split, nsplit, tile_sz, llo, lhi, *w);
+      for (int s = 0; s < FE_NSTAGE; ++s) mbar_init(&bar[s], 1);
+      mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int i = 0; i < FE_NSTAGE && i < w->total; ++i) issue(i);
+  }
+  FE_DEV void issue(int i) const {
+    int L, first, n;
+    fe_item(*w, tile_sz, i, L, first, n);
+    const int s = i % FE_NSTAGE;
+    const unsigned bytes = unsigned(n) * unsigned(rec[L]) * unsigned(elem);
+    const unsigned bytes2 = rec2 ? unsigned(n) * unsigned(rec2[L]) * unsigned(elem2) : 0u;
+    mbar_expect_tx(&bar[s], bytes + bytes2);
+    bulk_g2s(smem + s * FE_STAGE_BYTES, table + off[L] + size_t(first) * rec[L] * elem, bytes,
+             &bar[s]);
+    if (rec2)
+      bulk_g2s(smem + s * FE_STAGE_BYTES + bytes, table + off2[L] + size_t(first) * rec2[L] * elem2,
+               bytes2, &bar[s]);
+  }
+  // Wait for tile i; false (for every thread) if the wait gave up.
+  FE_DEV bool wait(int i) const {
+    const bool got = mbar_wait_bounded(&bar[i % FE_NSTAGE], (i / FE_NSTAGE) & 1);
+    return !__syncthreads_or(!got);
+  }
+  FE_DEV const unsigned char* stage(int i) const { return smem + (i % FE_NSTAGE) * FE_STAGE_BYTES; }
+  FE_DEV void release(int i) const {
+    __syncthreads();
+    if (threadIdx.x == 0 && i + FE_NSTAGE < w->total) issue(i + FE_NSTAGE);
+  }
+  // After a failed wait at tile i: drain the copies still in flight.
+  FE_DEV void abort(int i) const {
+    if (threadIdx.x == 0)
+      for (int k = i + 1; k < i + FE_NSTAGE && k < w->total; ++k)
+        mbar_wait_bounded(&bar[k % FE_NSTAGE], (k / FE_NSTAGE) & 1);
+    __syncthreads();
+  }
+};
 
 template <int L, int NP>
 FE_DEV void fe_tile_f64(const double* __restrict__ rec, int n, const double (&cx)[NP],
@@ -97,7 +156,7 @@ FE_DEV void fe_tile_f64(const double* __restrict__ rec, int n, const double (&cx
       const double T = pe * fma(x[j], x[j], fma(y[j], y[j], z[j] * z[j]));
       fe_boys_f64<L>(T, F[j]);
     }
-    fe_poly<L, double, NP>(rec + 5, x, y, z, F, s);
+    fe_poly<L, double, NP>(FeCoef<double>{rec + 6}, x, y, z, F, s);
 #pragma unroll
     for (int j = 0; j < NP; ++j) acc[j] = fma(K, s[j], acc[j]);
   }
@@ -113,10 +172,11 @@ FE_DEV double fe_nuclear(const double* __restrict__ Z, const double* __restrict_
   return v;
 }
 
-template <int NP, int NT>
-__global__ void __launch_bounds__(NT) fe_eval_f64_kernel(const FeEvalArgs a) {
+template <int NP, int NT, int MINB, int LLO, int LHI>
+__global__ void __launch_bounds__(NT, MINB) fe_eval_f64_kernel(const FeEvalArgs a) {
   extern __shared__ __align__(128) unsigned char fe_smem[];
   __shared__ uint64_t full_bar[FE_NSTAGE];
+  __shared__ FeBlockWork w;
   const FeTableHdr* hdr = reinterpret_cast<const FeTableHdr*>(a.table);
   const int tid = threadIdx.x;
   const int split = blockIdx.y;
@@ -124,84 +184,36 @@ __global__ void __launch_bounds__(NT) fe_eval_f64_kernel(const FeEvalArgs a) {
   // this thread's points (strided for coalesced loads); out-of-range lanes
   // evaluate a copy of the last point and store nothing
   double cx[NP], cy[NP], cz[NP], acc[NP];
-  int pidx[NP];
 #pragma unroll
   for (int j = 0; j < NP; ++j) {
-    pidx[j] = blockIdx.x * (NT * NP) + j * NT + tid;
-    const int q = min(pidx[j], a.npts - 1);
+    const int q = min(int(blockIdx.x) * (NT * NP) + j * NT + tid, a.npts - 1);
     cx[j] = a.pts[3 * q];
     cy[j] = a.pts[3 * q + 1];
     cz[j] = a.pts[3 * q + 2];
     acc[j] = 0.0;
   }
-
-  int tile_sz[FE_NCLASS];
-#pragma unroll
-  for (int L = 0; L < FE_NCLASS; ++L) tile_sz[L] = fe_c_tile64[L];
-  FeBlockWork w;
-  fe_block_work(hdr, split, a.nsplit, tile_sz, w);
-
-  if (tid == 0) {
-    for (int s = 0; s < FE_NSTAGE; ++s) mbar_init(&full_bar[s], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-
-  auto issue = [&](int i) {
-    int L, first, n;
-    fe_item(hdr, w, split, a.nsplit, tile_sz, i, L, first, n);
-    const int s = i % FE_NSTAGE;
-    const unsigned bytes = unsigned(n) * unsigned(fe_c_rec64[L]) * 8u;
-    const unsigned char* src = a.table + hdr->off64[L] + size_t(first) * fe_c_rec64[L] * 8;
-    mbar_expect_tx(&full_bar[s], bytes);
-    bulk_g2s(fe_smem + s * FE_STAGE_BYTES, src, bytes, &full_bar[s]);
-  };
-  if (tid == 0)
-    for (int i = 0; i < FE_NSTAGE && i < w.total; ++i) issue(i);
-
-  bool ok = true;
-  int i = 0;
-  for (; i < w.total; ++i) {
-    const int s = i % FE_NSTAGE;
-    const bool got = mbar_wait_bounded(&full_bar[s], (i / FE_NSTAGE) & 1);
-    if (__syncthreads_or(!got)) { ok = false; break; }
-    int L, first, n;
-    fe_item(hdr, w, split, a.nsplit, tile_sz, i, L, first, n);
-    const double* rec = reinterpret_cast<const double*>(fe_smem + s * FE_STAGE_BYTES);
-    switch (L) {
-      case 0: fe_tile_f64<0, NP>(rec, n, cx, cy, cz, acc); break;
-      case 1: fe_tile_f64<1, NP>(rec, n, cx, cy, cz, acc); break;
-      case 2: fe_tile_f64<2, NP>(rec, n, cx, cy, cz, acc); break;
-      case 3: fe_tile_f64<3, NP>(rec, n, cx, cy, cz, acc); break;
-      case 4: fe_tile_f64<4, NP>(rec, n, cx, cy, cz, acc); break;
-      case 5: fe_tile_f64<5, NP>(rec, n, cx, cy, cz, acc); break;
-      case 6: fe_tile_f64<6, NP>(rec, n, cx, cy, cz, acc); break;
-      case 7: fe_tile_f64<7, NP>(rec, n, cx, cy, cz, acc); break;
-      case 8: fe_tile_f64<8, NP>(rec, n, cx, cy, cz, acc); break;
-      default: fe_flag(FE_ST_BADCLASS); break;
+  FeTilePipe pipe{a.table, fe_c_tile64, fe_c_rec64, hdr->off64, 8, fe_smem, full_bar, &w};
+  pipe.start(hdr, split, a.nsplit, LLO, LHI);
+  const int total = w.total;
+  for (int i = 0; i < total; ++i) {
+    if (!pipe.wait(i)) {
+      pipe.abort(i);
+      return;
     }
-    __syncthreads();                       // stage s fully consumed
-    if (tid == 0 && i + FE_NSTAGE < w.total) issue(i + FE_NSTAGE);
-  }
-  if (!ok) {
-    // drain copies still in flight before the block's shared memory goes away
-    if (tid == 0)
-      for (int k = i + 1; k < i + FE_NSTAGE && k < w.total; ++k)
-        mbar_wait_bounded(&full_bar[k % FE_NSTAGE], (k / FE_NSTAGE) & 1);
-    __syncthreads();
-    return;
+    int L, first, n;
+    fe_item(w, fe_c_tile64, i, L, first, n);
+    const double* rec = reinterpret_cast<const double*>(pipe.stage(i));
+#define FE_C64(l) if (l >= LLO && l <= LHI && L == l) fe_tile_f64<(l >= LLO && l <= LHI ? l : LLO), NP>(rec, n, cx, cy, cz, acc);
+    FE_C64(0) FE_C64(1) FE_C64(2) FE_C64(3) FE_C64(4) FE_C64(5) FE_C64(6) FE_C64(7) FE_C64(8)
+#undef FE_C64
+    if (L < LLO || L > LHI) fe_flag(FE_ST_BADCLASS);
+    pipe.release(i);
   }
 
-  const double* Z = reinterpret_cast<const double*>(a.table + hdr->off_atoms);
-  const double* xyz = Z + hdr->n_atoms;
 #pragma unroll
   for (int j = 0; j < NP; ++j) {
-    if (pidx[j] >= a.npts) continue;
-    if (a.nsplit == 1)
-      a.out[pidx[j]] = a.mode == 1 ? acc[j]
-                                   : fe_nuclear(Z, xyz, hdr->n_atoms, cx[j], cy[j], cz[j]) - acc[j];
-    else
-      a.partial[size_t(split) * a.ld + pidx[j]] = acc[j];
+    const int p = int(blockIdx.x) * (NT * NP) + j * NT + tid;
+    if (p < a.npts) a.partial[size_t(split) * a.ld + p] = acc[j];
   }
 }
 

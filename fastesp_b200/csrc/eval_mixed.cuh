@@ -1,0 +1,309 @@
+// Mixed-precision ESP evaluation (same result as eval_f64 to <= 1e-6 a.u.).
+//
+// FP32 for the per-pair Boys vector, the monomial/Horner polynomial and the
+// products; FP64 where FP32 would not hold the error budget:
+//
+//  * routing: for every pair and every point the bound K*bound/|R| (the
+//    reference's screening bound, fastesp/esp.py:251-254, evaluated at the
+//    point) bounds sum_k |G_k R^a F_m|; when it reaches ``tau`` for any point
+//    of a warp's point set, that (pair, warp) is evaluated in FP64 instead.
+//    Two kernels share the bit-identical FP32 routing test (fe_route):
+//    fe_eval_f32_kernel evaluates every (pair, warp) the test leaves in FP32
+//    and skips the rest; fe_eval_fix64_kernel evaluates exactly the skipped
+//    ones in FP64.  Neither carries the other's code, so each keeps its
+//    registers, and no state passes between them.  1/|R| comes from the
+//    rsqrt that the FP32 Boys function needs anyway (T^-1/2 = p^-1/2 / |R|).
+//  * R = C - P from float hi/lo splits of both coordinates, so R carries about
+//    one float ulp of R itself rather than of |C|.
+//  * accumulation: FP32 contributions into a compensated two-sum pair per
+//    point (TwoSum: Knuth, The Art of Computer Programming vol. 2, 4.2.2), FP64
+//    contributions into an FP64 sum; the splits, the nuclear term and the final
+//    nuclear - electron subtraction are FP64.
+//
+// Grid and pipeline as eval_f64: points in registers (NP per thread), record
+// tiles streamed to shared memory by 1-D TMA bulk copies over an mbarrier ring.
+// Both kernels use the same point blocks (FE_MX_NT threads x FE_MX_NP points),
+// so a warp covers the same points in both and the routing votes agree.
+#pragma once
+#include "eval_f64.cuh"
+
+#ifndef FE_MX_NP
+#define FE_MX_NP 4            // points per thread of both mixed kernels
+#endif
+#define FE_MX_NT 128          // threads per block of both mixed kernels
+
+struct FeMixedArgs {
+  const unsigned char* table;
+  const double* pts;
+  int npts;
+  int nsplit;
+  double* partial;               // [nsplit][ld] partial electron sums of this kernel
+  int ld;
+  float tau;                     // FP64 routing threshold (a.u.)
+  unsigned long long* n64;       // optional: count of (pair, warp) FP64 evaluations
+};
+
+__constant__ int fe_c_tile32[FE_NCLASS] = {
+  FE_STAGE_BYTES / (4 * fe_class_rec32[0]), FE_STAGE_BYTES / (4 * fe_class_rec32[1]),
+  FE_STAGE_BYTES / (4 * fe_class_rec32[2]), FE_STAGE_BYTES / (4 * fe_class_rec32[3]),
+  FE_STAGE_BYTES / (4 * fe_class_rec32[4]), FE_STAGE_BYTES / (4 * fe_class_rec32[5]),
+  FE_STAGE_BYTES / (4 * fe_class_rec32[6]), FE_STAGE_BYTES / (4 * fe_class_rec32[7]),
+  FE_STAGE_BYTES / (4 * fe_class_rec32[8])};
+
+// Pairs per stage of the FP64-part kernel: routing record + FP64 record.
+__constant__ int fe_c_tilefix[FE_NCLASS] = {
+  FE_STAGE_BYTES / (4 * fe_class_rec32[0] + 8 * fe_class_rec64[0]),
+  FE_STAGE_BYTES / (4 * fe_class_rec32[1] + 8 * fe_class_rec64[1]),
+  FE_STAGE_BYTES / (4 * fe_class_rec32[2] + 8 * fe_class_rec64[2]),
+  FE_STAGE_BYTES / (4 * fe_class_rec32[3] + 8 * fe_class_rec64[3]),
+  FE_STAGE_BYTES / (4 * fe_class_rec32[4] + 8 * fe_class_rec64[4]),
+  FE_STAGE_BYTES / (4 * fe_class_rec32[5] + 8 * fe_class_rec64[5]),
+  FE_STAGE_BYTES / (4 * fe_class_rec32[6] + 8 * fe_class_rec64[6]),
+  FE_STAGE_BYTES / (4 * fe_class_rec32[7] + 8 * fe_class_rec64[7]),
+  FE_STAGE_BYTES / (4 * fe_class_rec32[8] + 8 * fe_class_rec64[8])};
+
+FE_DEV void fe_two_sum(float& hi, float& lo, float b) {
+  const float s = hi + b;
+  const float bb = s - hi;
+  const float err = (hi - (s - bb)) + (b - bb);
+  hi = s;
+  lo += err;
+}
+
+// The routing test of one pair for this thread's points; identical in both
+// kernels (explicit fmaf, MUFU rsqrt), so their warp votes agree bit for bit.
+template <int NP>
+FE_DEV bool fe_route(const float* __restrict__ rec, const float (&cxh)[NP], const float (&cyh)[NP],
+                     const float (&czh)[NP], const float (&cxl)[NP], const float (&cyl)[NP],
+                     const float (&czl)[NP], float (&x)[NP], float (&y)[NP], float (&z)[NP],
+                     float (&r2)[NP], float (&ir)[NP], float tau) {
+  const float kb = rec[10];
+  bool need = false;
+#pragma unroll
+  for (int j = 0; j < NP; ++j) {
+    x[j] = __fadd_rn(__fsub_rn(cxh[j], rec[2]), __fsub_rn(cxl[j], rec[5]));
+    y[j] = __fadd_rn(__fsub_rn(cyh[j], rec[3]), __fsub_rn(cyl[j], rec[6]));
+    z[j] = __fadd_rn(__fsub_rn(czh[j], rec[4]), __fsub_rn(czl[j], rec[7]));
+    r2[j] = fmaf(x[j], x[j], fmaf(y[j], y[j], __fmul_rn(z[j], z[j])));
+    ir[j] = rsqrtf(r2[j]);
+    need |= !(__fmul_rn(kb, ir[j]) < tau);
+  }
+  return __any_sync(0xffffffffu, need);
+}
+
+// Bounding sphere of the warp's points (from the float coordinates), equal in
+// every lane.  The radius carries a 1e-3 Bohr margin.
+template <int NP>
+FE_DEV void fe_warp_sphere(const float (&cxh)[NP], const float (&cyh)[NP], const float (&czh)[NP],
+                           float& ox, float& oy, float& oz, float& rad) {
+  float sx = 0.f, sy = 0.f, sz = 0.f;
+#pragma unroll
+  for (int j = 0; j < NP; ++j) { sx += cxh[j]; sy += cyh[j]; sz += czh[j]; }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sx += __shfl_xor_sync(0xffffffffu, sx, o);
+    sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    sz += __shfl_xor_sync(0xffffffffu, sz, o);
+  }
+  ox = sx * (1.0f / (32 * NP));
+  oy = sy * (1.0f / (32 * NP));
+  oz = sz * (1.0f / (32 * NP));
+  float r2 = 0.f;
+#pragma unroll
+  for (int j = 0; j < NP; ++j) {
+    const float dx = cxh[j] - ox, dy = cyh[j] - oy, dz = czh[j] - oz;
+    r2 = fmaxf(r2, dx * dx + dy * dy + dz * dz);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) r2 = fmaxf(r2, __shfl_xor_sync(0xffffffffu, r2, o));
+  rad = sqrtf(r2) + 1e-3f;
+}
+
+// True when no point of the warp can be routed to FP64 for this pair: every
+// point lies farther than its routing radius K*bound/tau (with a 0.1% + 1e-3
+// Bohr margin, far above the float rounding of the per-point test, so that
+// fe_route would also have answered "FP32" for every point).
+FE_DEV bool fe_out_of_reach(const float* __restrict__ rec, float ox, float oy, float oz,
+                            float rad, float inv_tau) {
+  const float dx = rec[2] - ox, dy = rec[3] - oy, dz = rec[4] - oz;
+  const float d = sqrtf(dx * dx + dy * dy + dz * dz) - rad;
+  const float reach = rec[10] * inv_tau * 1.001f + 1e-3f;
+  return d > reach;
+}
+
+template <int NP>
+FE_DEV void fe_load_points_split(const double* __restrict__ pts, int npts, int p0, int stride,
+                                 float (&cxh)[NP], float (&cyh)[NP], float (&czh)[NP],
+                                 float (&cxl)[NP], float (&cyl)[NP], float (&czl)[NP]) {
+#pragma unroll
+  for (int j = 0; j < NP; ++j) {
+    const int q = min(p0 + j * stride, npts - 1);
+    const double c0 = pts[3 * q], c1 = pts[3 * q + 1], c2 = pts[3 * q + 2];
+    cxh[j] = float(c0); cxl[j] = float(c0 - double(cxh[j]));
+    cyh[j] = float(c1); cyl[j] = float(c1 - double(cyh[j]));
+    czh[j] = float(c2); czl[j] = float(c2 - double(czh[j]));
+  }
+}
+
+// FP32 evaluation of a tile, skipping the (pair, warp) routed to FP64.
+template <int L, int NP>
+FE_DEV void fe_tile_f32(const float* __restrict__ rec, int n,
+                        const float (&cxh)[NP], const float (&cyh)[NP], const float (&czh)[NP],
+                        const float (&cxl)[NP], const float (&cyl)[NP], const float (&czl)[NP],
+                        float (&ahi)[NP], float (&alo)[NP], const float* __restrict__ grid,
+                        float tau) {
+  constexpr int S32 = fe_class_rec32[L];
+#pragma unroll 1
+  for (int i = 0; i < n; ++i, rec += S32) {
+    float x[NP], y[NP], z[NP], r2[NP], ir[NP];
+    if (fe_route<NP>(rec, cxh, cyh, czh, cxl, cyl, czl, x, y, z, r2, ir, tau)) continue;
+    const float pe = rec[0], rsp = rec[11], K = rec[8];
+    float F[NP][L + 1], s[NP];
+#pragma unroll
+    for (int j = 0; j < NP; ++j) fe_boys_f32<L>(pe * r2[j], ir[j] * rsp, grid, F[j]);
+    fe_poly<L, float, NP>(FeCoef<float>{rec + 12}, x, y, z, F, s);
+#pragma unroll
+    for (int j = 0; j < NP; ++j) fe_two_sum(ahi[j], alo[j], K * s[j]);
+  }
+}
+
+// FP64 evaluation of exactly the (pair, warp) the routing test sends to FP64.
+// ``rec`` is the tile's routing (mixed) records, ``rec64`` the same pairs'
+// FP64 records; points are evaluated two at a time for instruction-level
+// parallelism.
+template <int L, int NP>
+FE_DEV void fe_tile_fix64(const float* __restrict__ rec, const double* __restrict__ rec64, int n,
+                          const float (&cxh)[NP], const float (&cyh)[NP], const float (&czh)[NP],
+                          const float (&cxl)[NP], const float (&cyl)[NP], const float (&czl)[NP],
+                          const double (&cx)[NP], const double (&cy)[NP], const double (&cz)[NP],
+                          double (&a64)[NP], float tau, float ox, float oy, float oz, float rad,
+                          unsigned& n64) {
+  static_assert(NP % 2 == 0, "points are evaluated in pairs");
+  constexpr int S32 = fe_class_rec32[L];
+  constexpr int S64 = fe_class_rec64[L];
+  const float inv_tau = 1.0f / tau;
+#pragma unroll 1
+  for (int i = 0; i < n; ++i, rec += S32, rec64 += S64) {
+    if (fe_out_of_reach(rec, ox, oy, oz, rad, inv_tau)) continue;   // warp-uniform
+    float x[NP], y[NP], z[NP], r2[NP], ir[NP];
+    if (!fe_route<NP>(rec, cxh, cyh, czh, cxl, cyl, czl, x, y, z, r2, ir, tau)) continue;
+    ++n64;
+    const double pe = rec64[0], px = rec64[1], py = rec64[2], pz = rec64[3], K = rec64[4];
+#pragma unroll 1
+    for (int h = 0; h < NP; h += 2) {
+      double xx[2], yy[2], zz[2], F[2][L + 1], s[2];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        xx[j] = cx[h + j] - px;
+        yy[j] = cy[h + j] - py;
+        zz[j] = cz[h + j] - pz;
+        fe_boys_f64<L>(pe * fma(xx[j], xx[j], fma(yy[j], yy[j], zz[j] * zz[j])), F[j]);
+      }
+      fe_poly<L, double, 2>(FeCoef<double>{rec64 + 6}, xx, yy, zz, F, s);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) a64[h + j] = fma(K, s[j], a64[h + j]);
+    }
+  }
+}
+
+// Dispatch on the tile's class among the compiled range [LLO, LHI] only.
+#define FE_IN(l) ((l) >= LLO && (l) <= LHI ? (l) : LLO)
+#define FE_MX_SWITCH(CALL)                                                        \
+  if (L < LLO || L > LHI) fe_flag(FE_ST_BADCLASS);                                \
+  if (0 >= LLO && 0 <= LHI && L == 0) CALL(FE_IN(0));                             \
+  if (1 >= LLO && 1 <= LHI && L == 1) CALL(FE_IN(1));                             \
+  if (2 >= LLO && 2 <= LHI && L == 2) CALL(FE_IN(2));                             \
+  if (3 >= LLO && 3 <= LHI && L == 3) CALL(FE_IN(3));                             \
+  if (4 >= LLO && 4 <= LHI && L == 4) CALL(FE_IN(4));                             \
+  if (5 >= LLO && 5 <= LHI && L == 5) CALL(FE_IN(5));                             \
+  if (6 >= LLO && 6 <= LHI && L == 6) CALL(FE_IN(6));                             \
+  if (7 >= LLO && 7 <= LHI && L == 7) CALL(FE_IN(7));                             \
+  if (8 >= LLO && 8 <= LHI && L == 8) CALL(FE_IN(8));
+
+template <int MINB, int LLO, int LHI>
+__global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMixedArgs a) {
+  constexpr int NP = FE_MX_NP, NT = FE_MX_NT;
+  extern __shared__ __align__(128) unsigned char fe_smem[];
+  __shared__ uint64_t full_bar[FE_NSTAGE];
+  __shared__ FeBlockWork w;
+  __shared__ float grid[FE_BOYS32_NROW * FE_BOYS32_NTAB];
+  const FeTableHdr* hdr = reinterpret_cast<const FeTableHdr*>(a.table);
+  const int tid = threadIdx.x;
+  for (int k = tid; k < FE_BOYS32_NROW * FE_BOYS32_NTAB; k += NT) grid[k] = fe_boys_grid32[k];
+  float cxh[NP], cyh[NP], czh[NP], cxl[NP], cyl[NP], czl[NP], ahi[NP], alo[NP];
+  const int p0 = int(blockIdx.x) * (NT * NP) + tid;
+  fe_load_points_split<NP>(a.pts, a.npts, p0, NT, cxh, cyh, czh, cxl, cyl, czl);
+#pragma unroll
+  for (int j = 0; j < NP; ++j) ahi[j] = alo[j] = 0.0f;
+  FeTilePipe pipe{a.table, fe_c_tile32, fe_c_rec32, hdr->off32, 4, fe_smem, full_bar, &w};
+  pipe.start(hdr, blockIdx.y, a.nsplit, LLO, LHI);
+  const int total = w.total;
+  for (int i = 0; i < total; ++i) {
+    if (!pipe.wait(i)) {
+      pipe.abort(i);
+      return;
+    }
+    int L, first, n;
+    fe_item(w, fe_c_tile32, i, L, first, n);
+    const float* rec = reinterpret_cast<const float*>(pipe.stage(i));
+#define FE_CALL32(l) fe_tile_f32<l, NP>(rec, n, cxh, cyh, czh, cxl, cyl, czl, ahi, alo, grid, a.tau)
+    FE_MX_SWITCH(FE_CALL32)
+#undef FE_CALL32
+    pipe.release(i);
+  }
+#pragma unroll
+  for (int j = 0; j < NP; ++j) {
+    const int p = p0 + j * NT;
+    if (p < a.npts) a.partial[size_t(blockIdx.y) * a.ld + p] = double(ahi[j]) + double(alo[j]);
+  }
+}
+
+template <int MINB, int LLO, int LHI>
+__global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_fix64_kernel(const FeMixedArgs a) {
+  constexpr int NP = FE_MX_NP, NT = FE_MX_NT;
+  extern __shared__ __align__(128) unsigned char fe_smem[];
+  __shared__ uint64_t full_bar[FE_NSTAGE];
+  __shared__ FeBlockWork w;
+  const FeTableHdr* hdr = reinterpret_cast<const FeTableHdr*>(a.table);
+  const int tid = threadIdx.x;
+  float cxh[NP], cyh[NP], czh[NP], cxl[NP], cyl[NP], czl[NP];
+  double cx[NP], cy[NP], cz[NP], a64[NP];
+  const int p0 = int(blockIdx.x) * (NT * NP) + tid;
+  fe_load_points_split<NP>(a.pts, a.npts, p0, NT, cxh, cyh, czh, cxl, cyl, czl);
+#pragma unroll
+  for (int j = 0; j < NP; ++j) {
+    const int q = min(p0 + j * NT, a.npts - 1);
+    cx[j] = a.pts[3 * q];
+    cy[j] = a.pts[3 * q + 1];
+    cz[j] = a.pts[3 * q + 2];
+    a64[j] = 0.0;
+  }
+  float ox, oy, oz, rad;
+  fe_warp_sphere<NP>(cxh, cyh, czh, ox, oy, oz, rad);
+  unsigned n64 = 0;
+  FeTilePipe pipe{a.table, fe_c_tilefix, fe_c_rec32, hdr->off32, 4, fe_smem, full_bar, &w,
+                  fe_c_rec64, hdr->off64, 8};
+  pipe.start(hdr, blockIdx.y, a.nsplit, LLO, LHI);
+  const int total = w.total;
+  for (int i = 0; i < total; ++i) {
+    if (!pipe.wait(i)) {
+      pipe.abort(i);
+      return;
+    }
+    int L, first, n;
+    fe_item(w, fe_c_tilefix, i, L, first, n);
+    const float* rec = reinterpret_cast<const float*>(pipe.stage(i));
+    const double* rec64 = reinterpret_cast<const double*>(pipe.stage(i) + size_t(n) * fe_c_rec32[L] * 4);
+#define FE_CALL64(l) fe_tile_fix64<l, NP>(rec, rec64, n, cxh, cyh, czh, cxl, cyl, czl, cx, cy, cz, \
+                                          a64, a.tau, ox, oy, oz, rad, n64)
+    FE_MX_SWITCH(FE_CALL64)
+#undef FE_CALL64
+    pipe.release(i);
+  }
+  if (a.n64 && (tid & 31) == 0) atomicAdd(a.n64, (unsigned long long)n64);
+#pragma unroll
+  for (int j = 0; j < NP; ++j) {
+    const int p = p0 + j * NT;
+    if (p < a.npts) a.partial[size_t(blockIdx.y) * a.ld + p] = a64[j];
+  }
+}

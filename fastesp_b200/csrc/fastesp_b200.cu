@@ -17,6 +17,7 @@
 #include "boys.cuh"
 #include "table.cuh"
 #include "eval_f64.cuh"
+#include "eval_mixed.cuh"
 #include "build.cuh"
 #include "../../include/fastesp_b200.h"
 
@@ -56,19 +57,66 @@ int sm_count() {
 // ---------------------------------------------------------------------------
 // Evaluation launch geometry
 // ---------------------------------------------------------------------------
+// Points per thread and minimum resident blocks of 128 threads per SM of the
+// FP64 and mixed evaluators (defaults chosen by measurement on B200).
+#ifndef FE_NP64
+#define FE_NP64 2
+#endif
+#ifndef FE_MINB64
+#define FE_MINB64 3
+#endif
+#ifndef FE_MINB32
+#define FE_MINB32 4
+#endif
+#ifndef FE_MINBFIX
+#define FE_MINBFIX 4
+#endif
 constexpr int kEvalThreads = 128;
-constexpr int kEvalNP = 2;
+constexpr int kNP64 = FE_NP64, kMinB64 = FE_MINB64;
+constexpr int kNP32 = FE_MX_NP, kMinB32 = FE_MINB32, kMinBFix = FE_MINBFIX;
+
+// Class ranges of the two kernel instances of every evaluator: classes up to
+// FE_LSPLIT (s..f shell pairs) and the g-shell classes above it, compiled
+// separately so the common classes do not carry the registers of the largest.
+#define FE_LSPLIT 6
 
 struct EvalGeom {
-  int nblk_x, nsplit, ld;
+  int nblk_x, ld;
+  int split[4];        // splits of: main, high (, FP64 part main, FP64 part high)
+  int nkern;
+  size_t ws_rows() const {
+    size_t r = 0;
+    for (int k = 0; k < nkern; ++k) r += size_t(split[k]);
+    return r;
+  }
 };
 
-EvalGeom eval_geom(int npts, int pts_per_block) {
-  EvalGeom g;
-  g.nblk_x = (npts + pts_per_block - 1) / pts_per_block;
-  const int target = 3 * sm_count();
-  g.nsplit = std::max(1, std::min(256, (target + g.nblk_x - 1) / std::max(1, g.nblk_x)));
+// Point blocks x pair splits: about 8 waves of resident blocks for the main
+// instances, so the last partial wave costs little (splits capped at 256);
+// the g-class instances get a few splits (they are empty for s..f bases).
+// Every kernel writes its own rows of partial sums; one reduction adds all
+// rows in a fixed order.
+EvalGeom eval_geom(int npts, int mode) {
+  const int ppb = kEvalThreads * (mode == 1 ? kNP32 : kNP64);
+  EvalGeom g{};
+  g.nblk_x = (npts + ppb - 1) / ppb;
+  auto splits = [&](int minb) {
+    const int target = 8 * minb * sm_count();
+    return std::max(1, std::min(256, (target + g.nblk_x - 1) / std::max(1, g.nblk_x)));
+  };
+  const int hi_splits = std::max(1, std::min(8, sm_count() / std::max(1, g.nblk_x)));
   g.ld = (npts + 31) & ~31;
+  if (mode == 1) {
+    g.nkern = 4;
+    g.split[0] = splits(kMinB32);
+    g.split[1] = hi_splits;
+    g.split[2] = splits(kMinBFix);
+    g.split[3] = hi_splits;
+  } else {
+    g.nkern = 2;
+    g.split[0] = splits(kMinB64);
+    g.split[1] = hi_splits;
+  }
   return g;
 }
 
@@ -188,8 +236,15 @@ int fe_plan_create(const fe_basis* b, fe_plan** out) {
     s.fn0 = i;
     s.nprim = b->fn_nprim[i];
     const int nc = (s.l + 1) * (s.l + 2) / 2;
-    if (s.l > 4) { delete p; return fail(FE_ERR_UNSUPPORTED, "shell %zu has l=%d > 4", p->shells.size(), s.l); }
-    if (j - i != nc) { delete p; return fail(FE_ERR_ARG, "shell at function %d has %d functions, expected %d", i, j - i, nc); }
+    if (s.l > 4) {
+      const int rc = fail(FE_ERR_UNSUPPORTED, "shell %zu has l=%d > 4", p->shells.size(), s.l);
+      delete p;
+      return rc;
+    }
+    if (j - i != nc) {
+      delete p;
+      return fail(FE_ERR_ARG, "shell at function %d has %d functions, expected %d", i, j - i, nc);
+    }
     if (s.nprim <= 0 || s.nprim > 65535 || b->fn_off[i] < 0 || b->fn_off[i] + s.nprim > b->n_prim) {
       delete p; return fail(FE_ERR_ARG, "shell at function %d: bad primitive range", i);
     }
@@ -457,45 +512,79 @@ int fe_table_info_get(const void* d_table, fe_table_info* info, cudaStream_t st)
 
 size_t fe_eval_ws_bytes(int n_pts, int mode) {
   if (n_pts <= 0) return 256;
-  (void)mode;
-  const EvalGeom g = eval_geom(n_pts, kEvalThreads * kEvalNP);
-  return g.nsplit > 1 ? align256(size_t(g.nsplit) * g.ld * sizeof(double)) : 256;
+  const EvalGeom g = eval_geom(n_pts, mode == 1 ? 1 : 0);
+  return align256(g.ws_rows() * g.ld * sizeof(double));
 }
 
 }  // extern "C"
 
 namespace {
 
-int eval_f64(const char* who, const void* d_table, const double* d_pts, int n_pts,
-             double* d_out, void* d_ws, size_t ws_bytes, int mode, cudaStream_t st) {
+int eval_launch(const char* who, const void* d_table, const double* d_pts, int n_pts,
+                double* d_out, void* d_ws, size_t ws_bytes, int out_mode, int prec,
+                double tau, unsigned long long* d_n64, cudaStream_t st) {
   if (n_pts < 0) return fail(FE_ERR_ARG, "%s: n_pts < 0", who);
   if (n_pts == 0) return FE_OK;
   if (!d_table || !d_pts || !d_out) return fail(FE_ERR_ARG, "%s: null argument", who);
-  const EvalGeom g = eval_geom(n_pts, kEvalThreads * kEvalNP);
-  if (g.nsplit > 1 && (!d_ws || ws_bytes < size_t(g.nsplit) * g.ld * sizeof(double)))
+  const EvalGeom g = eval_geom(n_pts, prec);
+  if (!d_ws || ws_bytes < g.ws_rows() * g.ld * sizeof(double))
     return fail(FE_ERR_SIZE, "%s: workspace too small (need %zu bytes)", who,
-                fe_eval_ws_bytes(n_pts, 0));
-  FeEvalArgs a{};
-  a.table = static_cast<const unsigned char*>(d_table);
-  a.pts = d_pts;
-  a.npts = n_pts;
-  a.nsplit = g.nsplit;
-  a.partial = static_cast<double*>(d_ws);
-  a.ld = g.ld;
-  a.out = d_out;
-  a.mode = mode;
+                fe_eval_ws_bytes(n_pts, prec));
   const int smem = FE_NSTAGE * FE_STAGE_BYTES;
-  FE_CUDA(cudaFuncSetAttribute(fe_eval_f64_kernel<kEvalNP, kEvalThreads>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  fe_eval_f64_kernel<kEvalNP, kEvalThreads><<<dim3(g.nblk_x, g.nsplit), kEvalThreads, smem, st>>>(a);
-  FE_CUDA(cudaGetLastError());
-  if (g.nsplit > 1) {
-    fe_reduce_kernel<<<(n_pts + 255) / 256, 256, 0, st>>>(a.table, d_pts, n_pts, a.partial,
-                                                          g.nsplit, g.ld, d_out, mode);
+  double* rows = static_cast<double*>(d_ws);
+  auto next_rows = [&](int k) {
+    double* r = rows;
+    rows += size_t(g.split[k]) * g.ld;
+    return r;
+  };
+  const unsigned char* tb = static_cast<const unsigned char*>(d_table);
+  if (prec == 0) {
+    FeEvalArgs a{};
+    a.table = tb;
+    a.pts = d_pts;
+    a.npts = n_pts;
+    a.ld = g.ld;
+    auto k0 = fe_eval_f64_kernel<kNP64, kEvalThreads, kMinB64, 0, FE_LSPLIT>;
+    auto k1 = fe_eval_f64_kernel<kNP64, kEvalThreads, 1, FE_LSPLIT + 1, FE_NCLASS - 1>;
+    a.nsplit = g.split[0];
+    a.partial = next_rows(0);
+    FE_CUDA(cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k0<<<dim3(g.nblk_x, g.split[0]), kEvalThreads, smem, st>>>(a);
     FE_CUDA(cudaGetLastError());
+    a.nsplit = g.split[1];
+    a.partial = next_rows(1);
+    FE_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k1<<<dim3(g.nblk_x, g.split[1]), kEvalThreads, smem, st>>>(a);
+  } else {
+    FeMixedArgs a{};
+    a.table = tb;
+    a.pts = d_pts;
+    a.npts = n_pts;
+    a.ld = g.ld;
+    a.tau = float(tau);
+    a.n64 = d_n64;
+    auto f0 = fe_eval_f32_kernel<kMinB32, 0, FE_LSPLIT>;
+    auto f1 = fe_eval_f32_kernel<1, FE_LSPLIT + 1, FE_NCLASS - 1>;
+    auto x0 = fe_eval_fix64_kernel<kMinBFix, 0, FE_LSPLIT>;
+    auto x1 = fe_eval_fix64_kernel<1, FE_LSPLIT + 1, FE_NCLASS - 1>;
+    const void* ks[4] = {(const void*)f0, (const void*)f1, (const void*)x0, (const void*)x1};
+    for (int k = 0; k < 4; ++k) {
+      a.nsplit = g.split[k];
+      a.partial = next_rows(k);
+      FE_CUDA(cudaFuncSetAttribute(ks[k], cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      void* args[] = {&a};
+      FE_CUDA(cudaLaunchKernel(ks[k], dim3(g.nblk_x, g.split[k]), dim3(FE_MX_NT), args, smem, st));
+    }
   }
+  FE_CUDA(cudaGetLastError());
+  fe_reduce_kernel<<<(n_pts + 255) / 256, 256, 0, st>>>(tb, d_pts, n_pts, static_cast<double*>(d_ws),
+                                                        int(g.ws_rows()), g.ld, d_out, out_mode);
+  FE_CUDA(cudaGetLastError());
   return FE_OK;
 }
+
+// Default FP64 routing threshold of the mixed evaluator (a.u.).
+constexpr double kTauDefault = 0.05;
 
 }  // namespace
 
@@ -503,12 +592,30 @@ extern "C" {
 
 int fe_esp_fp64(const void* d_table, const double* d_pts, int n_pts, double* d_out,
                 void* d_ws, size_t ws_bytes, cudaStream_t st) {
-  return eval_f64("fe_esp_fp64", d_table, d_pts, n_pts, d_out, d_ws, ws_bytes, 0, st);
+  return eval_launch("fe_esp_fp64", d_table, d_pts, n_pts, d_out, d_ws, ws_bytes, 0, 0, 0.0,
+                     nullptr, st);
 }
 
 int fe_electron_fp64(const void* d_table, const double* d_pts, int n_pts, double* d_out,
                      void* d_ws, size_t ws_bytes, cudaStream_t st) {
-  return eval_f64("fe_electron_fp64", d_table, d_pts, n_pts, d_out, d_ws, ws_bytes, 1, st);
+  return eval_launch("fe_electron_fp64", d_table, d_pts, n_pts, d_out, d_ws, ws_bytes, 1, 0, 0.0,
+                     nullptr, st);
+}
+
+int fe_esp_mixed(const void* d_table, const double* d_pts, int n_pts, double* d_out,
+                 void* d_ws, size_t ws_bytes, double tau, unsigned long long* d_n64,
+                 cudaStream_t st) {
+  if (!(tau > 0.0)) tau = kTauDefault;
+  return eval_launch("fe_esp_mixed", d_table, d_pts, n_pts, d_out, d_ws, ws_bytes, 0, 1, tau,
+                     d_n64, st);
+}
+
+int fe_electron_mixed(const void* d_table, const double* d_pts, int n_pts, double* d_out,
+                      void* d_ws, size_t ws_bytes, double tau, unsigned long long* d_n64,
+                      cudaStream_t st) {
+  if (!(tau > 0.0)) tau = kTauDefault;
+  return eval_launch("fe_electron_mixed", d_table, d_pts, n_pts, d_out, d_ws, ws_bytes, 1, 1, tau,
+                     d_n64, st);
 }
 
 int fe_nuclear_fp64(const void* d_table, const double* d_pts, int n_pts, double* d_out,

@@ -31,6 +31,11 @@ TAYLOR_K = 8                   # Taylor terms of the tabulated branch
 GRID_H = 1.0 / 16.0            # grid spacing of the tabulated branch
 GRID_TMAX = 12.0               # tabulated branch covers 0 <= T < GRID_TMAX
 NTAB = MMAX + TAYLOR_K         # orders stored per grid row
+TAYLOR_K32 = 6                 # FP32 grid: Taylor terms
+GRID_H32 = 1.0 / 4.0           # FP32 grid spacing (truncation < 6e-9 relative)
+GRID_TMAX32 = 32.0             # FP32 grid covers 0 <= T < 32 (the FP32 asymptotic
+                               # thresholds of orders <= 6 lie below it)
+NTAB32 = MMAX + TAYLOR_K32
 VARS = ("x", "y", "z")
 
 
@@ -92,7 +97,7 @@ def poly_m_major(L):
     first = True
     for m in sorted(by_m):
         def coef(k):
-            return f"const Real g{k} = g[{k}];", f"g{k}"
+            return f"const Real g{k} = g({k});", f"g{k}"
         em.horner(by_m[m], 0, acc, coef)
         if first:
             em.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) s[j] = F[j][{m}] * ha[j];")
@@ -115,11 +120,11 @@ def poly_alpha_major(L):
         ks = by_a[a]
         lines = []
         k0, m0 = ks[0]
-        lines.append(f"const Real g{k0} = g[{k0}]; "
+        lines.append(f"const Real g{k0} = g({k0}); "
                      f"FE_UNROLL for (int j = 0; j < NP; ++j) hd[j] = g{k0} * F[j][{m0}];")
         em.nops += 1
         for k, m in ks[1:]:
-            lines.append(f"const Real g{k} = g[{k}]; "
+            lines.append(f"const Real g{k} = g({k}); "
                          f"FE_UNROLL for (int j = 0; j < NP; ++j) hd[j] = fe_fma(g{k}, F[j][{m}], hd[j]);")
             em.nops += 1
         return " ".join(lines), "hd[j]"
@@ -135,8 +140,8 @@ def poly_function(L):
     b = poly_alpha_major(L)
     em, tag = (a, "m-major") if a.nops <= b.nops else (b, "alpha-major")
     out = [f"// class L={L}: {H.n_terms(L)} terms, {em.nops} fused ops per point ({tag})",
-           "template <typename Real, int NP>",
-           f"__device__ __forceinline__ void fe_poly_L{L}(const Real* __restrict__ g,",
+           "template <typename Real, int NP, typename GL>",
+           f"__device__ __forceinline__ void fe_poly_L{L}(const GL& g,",
            "    const Real (&x)[NP], const Real (&y)[NP], const Real (&z)[NP],",
            f"    const Real (&F)[NP][{L + 1}], Real (&s)[NP]) {{",
            "  Real ha[NP], hb[NP], hc[NP], hd[NP];",
@@ -164,7 +169,7 @@ def grad_function(L):
             by_m.setdefault(m + shift, {})[(ax, ay, az)] = k
         first = True
         for m in sorted(by_m):
-            em.horner(by_m[m], 0, acc, lambda k: (f"const Real g{k}_{name}{m} = g[{k}];",
+            em.horner(by_m[m], 0, acc, lambda k: (f"const Real g{k}_{name}{m} = g({k});",
                                                  f"g{k}_{name}{m}"))
             op = (f"{name}[j] = F[j][{m}] * ha[j];" if first else
                   f"{name}[j] = fe_fma(F[j][{m}], ha[j], {name}[j]);")
@@ -185,7 +190,7 @@ def grad_function(L):
         for m in sorted(by_m):
             em.horner(by_m[m], 0, acc,
                       lambda kf, c=c, m=m: (f"const Real g{kf[0]}_d{c}{m} = "
-                                            f"Real({kf[1]}) * g[{kf[0]}];",
+                                            f"Real({kf[1]}) * g({kf[0]});",
                                             f"g{kf[0]}_d{c}{m}"))
             op = (f"{cname}[j] = F[j][{m}] * ha[j];" if first else
                   f"{cname}[j] = fe_fma(F[j][{m}], ha[j], {cname}[j]);")
@@ -194,8 +199,8 @@ def grad_function(L):
         if first:
             em.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) {cname}[j] = Real(0);")
     out = [f"// class L={L}: value, F_(m+1) companion sum and monomial derivatives",
-           "template <typename Real, int NP>",
-           f"__device__ __forceinline__ void fe_grad_L{L}(const Real* __restrict__ g,",
+           "template <typename Real, int NP, typename GL>",
+           f"__device__ __forceinline__ void fe_grad_L{L}(const GL& g,",
            "    const Real (&x)[NP], const Real (&y)[NP], const Real (&z)[NP],",
            f"    const Real (&F)[NP][{L + 2}], Real (&s)[NP], Real (&u)[NP],",
            "    Real (&dx)[NP], Real (&dy)[NP], Real (&dz)[NP]) {",
@@ -226,6 +231,14 @@ def boys_grid():
         T = mp.mpf(i) * mp.mpf(GRID_H)
         rows.append([float(boys_mp(n, T)) for n in range(NTAB)])
     return rows
+
+
+def boys_grid32():
+    import mpmath as mp
+    mp.mp.dps = 30
+    nrow = int(round(GRID_TMAX32 / GRID_H32)) + 2
+    return [[float(boys_mp(n, mp.mpf(i) * mp.mpf(GRID_H32))) for n in range(NTAB32)]
+            for i in range(nrow)]
 
 
 def asym_thresholds(rel=1e-16):
@@ -285,6 +298,22 @@ def main() -> int:
     out.append("// T above which the Boys vector F_0..F_M is its asymptotic form to 1e-16")
     out.append("static constexpr double fe_boys_asym_T[FE_MMAX + 1] = {"
                + ", ".join(repr(t) for t in ths) + "};")
+    th32 = asym_thresholds(rel=2e-8)
+    out.append("// the same for FP32 (2e-8 relative)")
+    out.append("static constexpr float fe_boys32_asym_T[FE_MMAX + 1] = {"
+               + ", ".join(repr(t) + "f" for t in th32) + "};")
+    out.append("")
+    rows32 = boys_grid32()
+    out.append(f"#define FE_BOYS32_NTAB {NTAB32}")
+    out.append(f"#define FE_BOYS32_TAYLOR_K {TAYLOR_K32}")
+    out.append(f"#define FE_BOYS32_GRID_INV_H {1.0 / GRID_H32!r}f")
+    out.append(f"#define FE_BOYS32_GRID_H {GRID_H32!r}f")
+    out.append(f"#define FE_BOYS32_GRID_TMAX {GRID_TMAX32!r}f")
+    out.append(f"#define FE_BOYS32_NROW {len(rows32)}")
+    out.append("__device__ const float fe_boys_grid32[FE_BOYS32_NROW * FE_BOYS32_NTAB] = {")
+    for r in rows32:
+        out.append("  " + ", ".join(repr(float(v)) + "f" if v > 1e-37 else "0.0f" for v in r) + ",")
+    out.append("};")
     out.append("")
     # Boys grid
     rows = boys_grid()
@@ -328,23 +357,37 @@ def main() -> int:
         out += grad_function(L)
         out.append("")
     # compile-time dispatch on the class
-    out.append("template <int L, typename Real, int NP>")
-    out.append("__device__ __forceinline__ void fe_poly(const Real* __restrict__ g,")
+    out.append("// g(k): coefficient k of the class's term list (a plain array or a split record)")
+    out.append("template <typename Real>")
+    out.append("struct FeCoef {")
+    out.append("  const Real* __restrict__ p;")
+    out.append("  __device__ __forceinline__ Real operator()(int k) const { return p[k]; }")
+    out.append("};")
+    out.append("struct FeCoefSplit {   // double from a float hi/lo pair")
+    out.append("  const float* __restrict__ hi;")
+    out.append("  const float* __restrict__ lo;")
+    out.append("  __device__ __forceinline__ double operator()(int k) const {")
+    out.append("    return double(hi[k]) + double(lo[k]);")
+    out.append("  }")
+    out.append("};")
+    out.append("")
+    out.append("template <int L, typename Real, int NP, typename GL>")
+    out.append("__device__ __forceinline__ void fe_poly(const GL& g,")
     out.append("    const Real (&x)[NP], const Real (&y)[NP], const Real (&z)[NP],")
     out.append("    const Real (&F)[NP][L + 1], Real (&s)[NP]) {")
     for L in range(LMAX + 1):
         kw = "if" if L == 0 else "else if"
-        out.append(f"  {kw} constexpr (L == {L}) fe_poly_L{L}<Real, NP>(g, x, y, z, F, s);")
+        out.append(f"  {kw} constexpr (L == {L}) fe_poly_L{L}<Real, NP, GL>(g, x, y, z, F, s);")
     out.append("}")
     out.append("")
-    out.append("template <int L, typename Real, int NP>")
-    out.append("__device__ __forceinline__ void fe_grad(const Real* __restrict__ g,")
+    out.append("template <int L, typename Real, int NP, typename GL>")
+    out.append("__device__ __forceinline__ void fe_grad(const GL& g,")
     out.append("    const Real (&x)[NP], const Real (&y)[NP], const Real (&z)[NP],")
     out.append("    const Real (&F)[NP][L + 2], Real (&s)[NP], Real (&u)[NP],")
     out.append("    Real (&dx)[NP], Real (&dy)[NP], Real (&dz)[NP]) {")
     for L in range(LMAX + 1):
         kw = "if" if L == 0 else "else if"
-        out.append(f"  {kw} constexpr (L == {L}) fe_grad_L{L}<Real, NP>(g, x, y, z, F, s, u, dx, dy, dz);")
+        out.append(f"  {kw} constexpr (L == {L}) fe_grad_L{L}<Real, NP, GL>(g, x, y, z, F, s, u, dx, dy, dz);")
     out.append("}")
     out.append("")
     out.append("__constant__ int fe_c_rec64[FE_NCLASS] = {"
@@ -355,7 +398,7 @@ def main() -> int:
                + ", ".join(map(str, nts)) + "};")
     (HERE / "classes_gen.cuh").write_text("\n".join(out) + "\n")
     print("classes_gen.cuh:", len(out), "lines; poly ops", nops, "terms", nts,
-          "asym T", ths)
+          "asym T", ths, "fp32 asym T", th32)
     return 0
 
 

@@ -6,14 +6,17 @@
 //                           [class 0 FP32 records]...[atoms: Z[n], xyz[3n]]
 //
 // Pairs are grouped by angular class L = la + lb.  A class-L FP64 record is
-// fe_class_rec64[L] doubles: [p, Px, Py, Pz, K, G_0 .. G_(nt-1), pad], so the
+// fe_class_rec64[L] doubles: [p, Px, Py, Pz, K, K*bound, G_0 .. G_(nt-1), pad]
+// (K*bound is the screening bound's numerator, +inf when unknown), so the
 // records of a tile are one contiguous, 16-byte-aligned run that a single
 // bulk copy moves into shared memory.  Within a class, pairs keep the order of
 // the reference builder: shell pairs (si <= sj) in shell order, then
 // primitive pairs with the primitive of shell si outer.
 //
-// FP32 records (mixed-precision evaluator) are fe_class_rec32[L] floats:
-// [p, Px_hi, Py_hi, Pz_hi, Px_lo, Py_lo, Pz_lo, K, G_0 ..] (pad to 16 bytes).
+// Mixed-precision records are fe_class_rec32[L] floats holding every FP64 value
+// v as hi = float(v), lo = float(v - hi):
+// [p_hi, p_lo, Px_hi, Py_hi, Pz_hi, Px_lo, Py_lo, Pz_lo, K_hi, K_lo, K*bound,
+//  p^-1/2, G_hi[0..nt), G_lo[0..nt), pad to 16 bytes].
 #pragma once
 #include <cstdint>
 

@@ -97,18 +97,21 @@ def n_terms(L: int) -> int:
 
 
 def record_stride(L: int) -> int:
-    """FP64 words per pair record [p, Px, Py, Pz, K, G_0..G_nt-1], padded to 16 bytes."""
-    n = 5 + n_terms(L)
+    """FP64 words per pair record [p, Px, Py, Pz, K, K*bound, G_0..G_nt-1], padded to 16 bytes."""
+    n = 6 + n_terms(L)
     return n + (n & 1)
 
 
 def record_stride_f32(L: int) -> int:
     """FP32 words per mixed-precision record, padded to 16 bytes.
 
-    [p, Px_hi, Py_hi, Pz_hi, Px_lo, Py_lo, Pz_lo, K, G_0..] with P split into
-    a float and its float residual so R = C - P is formed to ~1 ulp of R.
+    Every FP64 value v of the FP64 record is kept as a float pair
+    hi = float(v), lo = float(v - hi) (hi + lo carries ~48 bits of v):
+    [p_hi, p_lo, Px_hi, Py_hi, Pz_hi, Px_lo, Py_lo, Pz_lo, K_hi, K_lo, K*bound,
+    p^-1/2, G_hi[0..nt), G_lo[0..nt)].  The FP32 path reads the hi halves; the
+    FP64 fallback rebuilds the FP64 values from both halves.
     """
-    n = 8 + n_terms(L)
+    n = 12 + 2 * n_terms(L)
     return (n + 3) // 4 * 4
 
 

@@ -256,16 +256,19 @@ def molden_for(name: str, seed: int = 0, natom: int | None = None) -> Path:
     return path
 
 
-def load_workload(name: str, n_points: int, seed: int = 0, grid: bool = False,
-                  natom: int | None = None):
-    """(wfn, basis, density, points) of a synthetic workload, via the MOLDEN reader."""
+def load_workload(name: str, n_points: int, seed: int = 0, points_seed: int = 1,
+                  grid: bool = False, natom: int | None = None):
+    """(wfn, basis, density, points) of a synthetic workload, via the MOLDEN reader.
+
+    ``seed`` picks the molecule, ``points_seed`` the point sample.
+    """
     wfn = read_molden(molden_for(name, seed, natom))
     basis = Basis(wfn)
     dens = basis.density_matrix_cartesian()
     if grid:
-        pts = cubic_grid_points(wfn.coords, n_points, seed=seed)
+        pts = cubic_grid_points(wfn.coords, n_points, seed=points_seed)
     else:
-        pts = vdw_surface_points(wfn.symbols, wfn.coords, n_points, seed=seed)
+        pts = vdw_surface_points(wfn.symbols, wfn.coords, n_points, seed=points_seed)
     return wfn, basis, dens, pts
 
 

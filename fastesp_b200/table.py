@@ -148,7 +148,10 @@ class Plan:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            _lib.lib().fe_plan_destroy(h)
+            try:
+                _lib.lib().fe_plan_destroy(h)
+            except Exception:       # interpreter shutdown: module globals already gone
+                pass
             self._h = None
 
 
@@ -221,31 +224,52 @@ class PairTable:
         d = _to_dev(pts, self.device).reshape(-1, 3)
         return d, as_numpy
 
-    def esp(self, points=None, precision: str = "fp64"):
-        """nuclear - electron in Hartree/e (fastesp/table.py:102-104)."""
-        return self._eval(points, precision, mode=0)
+    def esp(self, points=None, precision: str = "fp64", tau: float = 0.0):
+        """nuclear - electron in Hartree/e (fastesp/table.py:102-104).
 
-    def electron(self, points=None, precision: str = "fp64"):
+        ``precision="mixed"`` uses the FP32/FP64 evaluator (``tau``: its FP64
+        routing threshold in a.u., 0 for the default).
+        """
+        return self._eval(points, precision, mode=0, tau=tau)
+
+    def electron(self, points=None, precision: str = "fp64", tau: float = 0.0):
         """int rho(r)/|r-C| dr (fastesp/table.py:73-93)."""
-        return self._eval(points, precision, mode=1)
+        return self._eval(points, precision, mode=1, tau=tau)
 
     def nuclear(self, points=None):
         """sum_A Z_A/|C-R_A| (fastesp/table.py:95-100)."""
         return self._eval(points, "fp64", mode=2)
 
-    def _eval(self, points, precision, mode):
+    def _eval(self, points, precision, mode, tau=0.0, n64=None):
         torch = _torch()
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"unknown precision {precision!r}")
         d, as_numpy = self._points(points)
         n = int(d.shape[0])
         out = torch.empty(n, dtype=torch.float64, device=self.device)
-        if precision != "fp64":
-            raise ValueError(f"unknown precision {precision!r}")
         L = _lib.lib()
-        ws = _empty_bytes(L.fe_eval_ws_bytes(n, 0), self.device)
-        fn = {0: L.fe_esp_fp64, 1: L.fe_electron_fp64, 2: L.fe_nuclear_fp64}[mode]
-        _lib.check(fn(_lib.ptr(self._buf), _lib.ptr(d), n, _lib.ptr(out), _lib.ptr(ws),
-                      ws.numel(), _lib.stream_ptr()))
+        s = _lib.stream_ptr()
+        if mode == 2:
+            _lib.check(L.fe_nuclear_fp64(_lib.ptr(self._buf), _lib.ptr(d), n, _lib.ptr(out),
+                                         None, 0, s))
+        elif precision == "fp64":
+            ws = _empty_bytes(L.fe_eval_ws_bytes(n, 0), self.device)
+            fn = L.fe_esp_fp64 if mode == 0 else L.fe_electron_fp64
+            _lib.check(fn(_lib.ptr(self._buf), _lib.ptr(d), n, _lib.ptr(out), _lib.ptr(ws),
+                          ws.numel(), s))
+        else:
+            ws = _empty_bytes(L.fe_eval_ws_bytes(n, 1), self.device)
+            fn = L.fe_esp_mixed if mode == 0 else L.fe_electron_mixed
+            _lib.check(fn(_lib.ptr(self._buf), _lib.ptr(d), n, _lib.ptr(out), _lib.ptr(ws),
+                          ws.numel(), float(tau), _lib.ptr(n64), s))
         return out.cpu().numpy() if as_numpy else out
+
+    def esp_stats(self, points=None, tau: float = 0.0):
+        """Mixed-precision ESP and the number of (pair, warp) evaluations routed to FP64."""
+        torch = _torch()
+        n64 = torch.zeros(1, dtype=torch.int64, device=self.device)
+        v = self._eval(points, "mixed", 0, tau=tau, n64=n64)
+        return v, int(n64.item())
 
     # -- export / import (pairs.bin) -----------------------------------
     def records(self, L: int) -> np.ndarray:
@@ -296,7 +320,7 @@ class PairTable:
             pp["mo_axis"].append(np.tile(axis, n))
             pp["tm_aidx"].append(np.tile(aidx, n))
             pp["tm_m"].append(np.tile(H.term_m(L), n))
-            pp["tm_g"].append(r[:, 5:5 + nt].ravel())
+            pp["tm_g"].append(r[:, 6:6 + nt].ravel())
             toff += nt * n
             moff += nm * n
         out = {}
@@ -378,7 +402,8 @@ class PairTable:
                 rec[:, 2] = a["pp_cy"][sel]
                 rec[:, 3] = a["pp_cz"][sel]
                 rec[:, 4] = a["pp_K"][sel]
-                rec[:, 5:5 + ntL] = a["tm_g"][toff]
+                rec[:, 5] = np.inf          # no screening bound in pairs.bin
+                rec[:, 6:6 + ntL] = a["tm_g"][toff]
             recs.append(rec)
         L_ = _lib.lib()
         cap = (C.c_int * NCLASS)(*counts)

@@ -123,7 +123,8 @@ int fe_table_make_f32(void* d_table, cudaStream_t stream);
 /* Copy the table header to the host (synchronises ``stream``). */
 int fe_table_info_get(const void* d_table, fe_table_info* info, cudaStream_t stream);
 
-/* Workspace bytes of an evaluation of n_pts points (mode 0 FP64, 1 mixed). */
+/* Workspace bytes of an evaluation of n_pts points (mode 0 FP64, 1 mixed);
+ * holds the per-split partial sums of the pair-split reduction. */
 size_t fe_eval_ws_bytes(int n_pts, int mode);
 
 /* V(C) = sum_A Z_A/|C-R_A| - sum_pairs K sum_k G_k R^alpha F_m(p R^2), all FP64,
@@ -132,6 +133,21 @@ size_t fe_eval_ws_bytes(int n_pts, int mode);
  * and PairTable.esp (fastesp/table.py:102-104). */
 int fe_esp_fp64(const void* d_table, const double* d_pts, int n_pts, double* d_out,
                 void* d_ws, size_t ws_bytes, cudaStream_t stream);
+
+/* Mixed precision: the Boys vector, monomials and term products in FP32 with a
+ * compensated (two-sum) FP32 accumulation per point; a pair is evaluated in
+ * FP64 for a warp of points whenever its bound K*bound/|R| reaches ``tau``
+ * (a.u.; <= 0 selects the default 0.05) for one of them; the split sums, the
+ * nuclear term and the final subtraction are FP64.  Same result as
+ * fe_esp_fp64 within 1e-6 a.u. on the tested systems.  ``d_n64`` (nullable)
+ * accumulates the number of (pair, warp) evaluations routed to FP64.  No
+ * counterpart in the reference, which is FP64 only. */
+int fe_esp_mixed(const void* d_table, const double* d_pts, int n_pts, double* d_out,
+                 void* d_ws, size_t ws_bytes, double tau, unsigned long long* d_n64,
+                 cudaStream_t stream);
+int fe_electron_mixed(const void* d_table, const double* d_pts, int n_pts, double* d_out,
+                      void* d_ws, size_t ws_bytes, double tau, unsigned long long* d_n64,
+                      cudaStream_t stream);
 
 /* The electron part alone, int rho(r)/|r-C| dr (fastesp/table.py:73-93), FP64. */
 int fe_electron_fp64(const void* d_table, const double* d_pts, int n_pts, double* d_out,

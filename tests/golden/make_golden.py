@@ -40,6 +40,7 @@ def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
     ap.add_argument("--quick", action="store_true", help="skip the 54-atom fixture")
+    ap.add_argument("--only", default="", help="comma list: boys,pair_types,prim,systems,frag54")
     a = ap.parse_args()
     sys.path.insert(0, a.reference)
     sys.path.insert(0, str(ROOT))
@@ -47,17 +48,31 @@ def main() -> int:
     from fastesp import esp as Resp, ints as Rints
     from fastesp_b200 import synth
 
+    only = set(filter(None, a.only.split(",")))
+    want = (lambda k: not only or k in only)
     build_pairs = ROOT / "oracle" / "_ref" / "build_pairs"
     if not build_pairs.exists():
         subprocess.run(["make", "-C", str(ROOT / "oracle"), "_ref/build_pairs",
                         f"REF={a.reference}"], check=True)
 
-    # ---- Boys ---------------------------------------------------------------
-    T = np.concatenate([[0.0, 1e-14, 1e-12, 1e-10, 1e-8], np.logspace(-6, 5, 221),
-                        np.linspace(0.0, 60.0, 241)[1:], [0.1, 1.0, 5.0, 30.0, 1e4]])
-    ms = np.arange(17)
-    F = np.array([[Rints.boys(int(m), t) for t in T] for m in ms])
-    np.savez_compressed(HERE / "boys.npz", T=T, m=ms, F=F)
+    # ---- Boys (reference values, plus 40-digit values of the same function) --
+    if want("boys"):
+        import mpmath as mp
+        mp.mp.dps = 40
+        T = np.concatenate([[0.0, 1e-14, 1e-12, 1e-10, 1e-8], np.logspace(-6, 5, 221),
+                            np.linspace(0.0, 60.0, 241)[1:], [0.1, 1.0, 5.0, 30.0, 1e4]])
+        ms = np.arange(17)
+        F = np.array([[Rints.boys(int(m), t) for t in T] for m in ms])
+
+        def exact(m, t):
+            if t == 0.0:
+                return 1.0 / (2 * m + 1)
+            a_ = mp.mpf(m) + mp.mpf(1) / 2
+            return float(mp.gammainc(a_, 0, mp.mpf(t)) / (2 * mp.power(mp.mpf(t), a_)))
+        F_exact = np.array([[exact(int(m), float(t)) for t in T] for m in ms[:10]])
+        np.savez_compressed(HERE / "boys.npz", T=T, m=ms, F=F, F_exact=F_exact)
+    if not want("pair_types") and not want("prim") and not want("systems") and not want("frag54"):
+        return 0
 
     # ---- per-L contraction tables -------------------------------------------
     d = {"a8": Rints.a_table(8)}

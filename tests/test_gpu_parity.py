@@ -30,12 +30,16 @@ def _device_status_clean():
 
 
 def test_boys_gpu_matches_reference(golden):
+    """Against 40-digit values: 4e-15 relative.  Against the reference's own
+    hypergeometric values: within that function's own error plus 4e-15."""
     g = golden("boys")
     for m in range(10):
         got = boys(m, g["T"])
+        ex = g["F_exact"][m]
+        rel = np.abs(got - ex) / np.abs(ex)
+        assert rel.max() < 4e-15, (m, g["T"][np.argmax(rel)], rel.max())
         ref = g["F"][m]
-        rel = np.abs(got - ref) / np.abs(ref)
-        assert rel.max() < 5e-15, (m, g["T"][np.argmax(rel)], rel.max())
+        assert (np.abs(got - ref) <= np.abs(ref - ex) + 4e-15 * np.abs(ex)).all()
 
 
 def _asym_thresholds():
@@ -54,7 +58,7 @@ def test_boys_gpu_regime_edges():
             T = np.array([np.nextafter(e, 0.0), e, np.nextafter(e, 1e9)])
             got = np.stack([boys(m, T) for m in range(M + 1)])
             ref = np.stack([O.boys(m, T) for m in range(M + 1)])
-            assert (np.abs(got - ref) / ref).max() < 5e-15, (M, e)
+            assert (np.abs(got - ref) / ref).max() < 4e-15 * (1 + M), (M, e)
 
 
 def _class_order(tab_arrays):
@@ -85,7 +89,7 @@ def test_build_matches_reference_table(tag, request):
         np.testing.assert_allclose(rec[:, 4], g["tab_pp_K"][rows], rtol=1e-13)
         nt = H.n_terms(L)
         off = g["tab_pp_off"][rows][:, None] + np.arange(nt)[None, :]
-        np.testing.assert_allclose(rec[:, 5:5 + nt], g["tab_tm_g"][off], rtol=0, atol=1e-13 * gmax)
+        np.testing.assert_allclose(rec[:, 6:6 + nt], g["tab_tm_g"][off], rtol=0, atol=1e-13 * gmax)
 
 
 @pytest.mark.parametrize("tag", ["small", "tz6"])
@@ -110,7 +114,7 @@ def test_native_rule_matches_reference_builder(tag, request):
 
 @pytest.fixture(scope="module")
 def frag54():
-    wfn, basis, P, _ = synth.load_workload("frag54", 10, seed=1)
+    wfn, basis, P, _ = synth.load_workload("frag54", 10, seed=0)
     return wfn, basis, P
 
 
@@ -157,11 +161,23 @@ def test_export_reference_format_table(tmp_path, small_system):
 
 
 def test_primitive_pair_integrals(golden):
+    """The reference's quadrature-pinned cases (its tests/test_integrals.py:72-85);
+    shells above g (l > 4) are outside this library's classes and must be refused."""
     g = golden("prim_integrals")
+    checked = 0
     for la, lb, v in zip(g["la"], g["lb"], g["value"]):
-        got = primitive_pair_integral(float(g["alpha"]), g["A"], tuple(la), float(g["beta"]),
-                                      g["B"], tuple(lb), g["C"])
-        assert got == pytest.approx(v, rel=1e-12, abs=1e-15)
+        args = (float(g["alpha"]), g["A"], tuple(la), float(g["beta"]), g["B"], tuple(lb), g["C"])
+        if max(sum(la), sum(lb)) > 4:
+            with pytest.raises(_lib.FeError, match=r"l=\d+ > 4"):
+                primitive_pair_integral(*args)
+            continue
+        assert primitive_pair_integral(*args) == pytest.approx(v, rel=1e-12, abs=1e-15)
+        checked += 1
+    assert checked == 10
+    for row in g["ss"]:
+        A, B, C, al, be, v = row[:3], row[3:6], row[6:9], row[9], row[10], row[11]
+        assert primitive_pair_integral(al, A, (0, 0, 0), be, B, (0, 0, 0), C) == \
+            pytest.approx(v, rel=1e-13)
 
 
 def test_edge_cases(small_system):
@@ -261,3 +277,86 @@ def test_full_size_translation_invariant(frag54_30k):
     v1 = build_table(wfn, basis, P, sub, tol=0.0).esp()
     v2 = build_table(w2, b2, P, sub + shift, tol=0.0).esp()
     assert np.abs(v1 - v2).max() < 1e-9
+
+
+# ---------------------------------------------------------------------------
+# mixed precision: FP32 Boys/polynomial with FP64 routing, <= 1e-6 a.u.
+# ---------------------------------------------------------------------------
+MIXED_TOL = 1e-6
+
+
+@pytest.mark.parametrize("tag", ["small", "tz6"])
+def test_mixed_small_systems(tag, request):
+    wfn, basis, P, g = request.getfixturevalue(f"{tag}_system")
+    tab = build_table(wfn, basis, g["density"], g["points"], tol=1e-12)
+    assert np.abs(tab.esp(precision="mixed") - g["esp_t12"]).max() <= MIXED_TOL
+    assert np.abs(tab.electron(precision="mixed") - g["electron_t12"]).max() <= MIXED_TOL
+
+
+def test_mixed_frag54_reference_points(frag54, golden):
+    wfn, basis, P = frag54
+    g = golden("frag54_300")
+    tab = build_table(wfn, basis, P, g["points"], tol=1e-12)
+    assert np.abs(tab.esp(precision="mixed") - g["esp_t12"]).max() <= MIXED_TOL
+
+
+def test_mixed_full_size_vs_fp64(frag54_30k):
+    """The 30000-point workload: max and RMS error of the mixed path against FP64."""
+    wfn, basis, P, pts = frag54_30k
+    tab = build_table(wfn, basis, P, pts, tol=1e-12)
+    v64 = tab.esp()
+    vmx, n64 = tab.esp_stats()
+    err = np.abs(vmx - v64)
+    print(f"mixed vs fp64: max {err.max():.3e} rms {np.sqrt((err ** 2).mean()):.3e}, "
+          f"FP64-routed (pair, warp) evaluations {n64}")
+    assert err.max() <= MIXED_TOL
+    np.testing.assert_array_equal(tab.esp(precision="mixed"), vmx)     # deterministic
+
+
+def test_mixed_routing_extremes(tz6_system):
+    """tau -> 0 routes every pair to FP64 (FP64 result); a huge tau is pure FP32."""
+    wfn, basis, P, g = tz6_system
+    tab = build_table(wfn, basis, g["density"], g["points"], tol=1e-12)
+    v64 = tab.esp()
+    all64, n_all = tab.esp_stats(tau=1e-300)
+    assert n_all > 0
+    assert np.abs(all64 - v64).max() <= 1e-11
+    none64, n_none = tab.esp_stats(tau=1e300)
+    assert n_none == 0
+    assert np.abs(none64 - v64).max() < 1e-3
+
+
+def test_mixed_imported_table_is_all_fp64(tmp_path, small_system):
+    """pairs.bin carries no screening bound, so the mixed path evaluates in FP64."""
+    wfn, basis, P, g = small_system
+    tab = build_table(wfn, basis, g["density"], g["points"], tol=1e-12)
+    tab.write(tmp_path / "pairs.bin")
+    back = PairTable.read(tmp_path / "pairs.bin")
+    np.testing.assert_allclose(back.esp(precision="mixed"), g["esp_t12"], rtol=0, atol=1e-11)
+
+
+@pytest.mark.parametrize("npts", [300, 30000])
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_every_workspace_row_is_written(frag54, npts, prec):
+    """Evaluate through the C ABI with the workspace filled with NaN: every
+    partial-sum row the reduction reads must have been written by a kernel."""
+    import torch
+    wfn, basis, P = frag54
+    pts = synth.vdw_surface_points(wfn.symbols, wfn.coords, npts, seed=7)
+    pd = torch.as_tensor(pts, device="cuda")
+    tab = build_table(wfn, basis, P, pts, tol=1e-12)
+    L = _lib.lib()
+    mode = 0 if prec == "fp64" else 1
+    nb = L.fe_eval_ws_bytes(npts, mode)
+    ws = torch.full((nb // 8,), float("nan"), dtype=torch.float64, device="cuda")
+    out = torch.full((npts,), float("nan"), dtype=torch.float64, device="cuda")
+    if prec == "fp64":
+        _lib.check(L.fe_esp_fp64(_lib.ptr(tab._buf), _lib.ptr(pd), npts, _lib.ptr(out),
+                                 _lib.ptr(ws), nb, _lib.stream_ptr()))
+    else:
+        _lib.check(L.fe_esp_mixed(_lib.ptr(tab._buf), _lib.ptr(pd), npts, _lib.ptr(out),
+                                  _lib.ptr(ws), nb, 0.0, None, _lib.stream_ptr()))
+    got = out.cpu().numpy()
+    assert np.isfinite(got).all()
+    ref = tab.esp(pts, precision=prec)
+    np.testing.assert_array_equal(got, ref)
