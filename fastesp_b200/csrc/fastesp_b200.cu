@@ -9,6 +9,7 @@
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -688,4 +689,63 @@ extern "C" int fe_peak_run(int fp64, long long iters, int blocks, void* d_out, c
     fe_peak_kernel<float><<<blocks, 256, 0, st>>>(iters, static_cast<float*>(d_out));
   FE_CUDA(cudaGetLastError());
   return FE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free FP64 evaluation.
+//
+// Some callers cannot allocate device memory: a host application or plugin
+// framework that owns the whole device-memory budget and only lends the
+// library its input and output buffers, or a binding of the reference's own
+// two-buffer interface (pair table and points in, potentials out), which has
+// no notion of a workspace.  fe_esp_fp64_noalloc serves them: its partial-sum
+// workspace is this file-scope device array instead of a caller buffer.  The
+// array is FE_NOALLOC_SCRATCH_BYTES on every GPU that loads the library and
+// stays allocated until the process exits.
+// ---------------------------------------------------------------------------
+#define FE_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define FE_NOALLOC_MAX_DEVICES 128
+
+static __device__ __align__(256) unsigned char fe_noalloc_scratch[FE_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[FE_NOALLOC_MAX_DEVICES] = {};
+
+// Device address of the scratch array on the current device; resolved once per
+// device (the host-side symbol is only a stand-in, never a device address).
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  FE_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= FE_NOALLOC_MAX_DEVICES)
+    return fail(FE_ERR_UNSUPPORTED, "fe_esp_fp64_noalloc: device ordinal %d too large", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    FE_CUDA(cudaGetSymbolAddress(&p, fe_noalloc_scratch));
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return FE_OK;
+}
+}  // namespace
+
+extern "C" size_t fe_noalloc_scratch_bytes(void) { return FE_NOALLOC_SCRATCH_BYTES; }
+
+extern "C" int fe_esp_fp64_noalloc(const void* d_table, const double* d_pts, int n_pts,
+                                   double* d_out, cudaStream_t st) {
+  if (n_pts < 0) return fail(FE_ERR_ARG, "fe_esp_fp64_noalloc: n_pts < 0");
+  if (n_pts == 0) return FE_OK;
+  if (!d_table || !d_pts || !d_out) return fail(FE_ERR_ARG, "fe_esp_fp64_noalloc: null argument");
+  const size_t need = fe_eval_ws_bytes(n_pts, 0);
+  if (need > FE_NOALLOC_SCRATCH_BYTES)
+    return fail(FE_ERR_SIZE,
+                "fe_esp_fp64_noalloc: %d points need %zu bytes of scratch, more than the "
+                "%u-byte static array; use fe_esp_fp64 with a caller workspace",
+                n_pts, need, FE_NOALLOC_SCRATCH_BYTES);
+  void* scratch = nullptr;
+  const int rc = noalloc_scratch(&scratch);
+  if (rc != FE_OK) return rc;
+  return eval_launch("fe_esp_fp64_noalloc", d_table, d_pts, n_pts, d_out, scratch, need, 0, 0,
+                     0.0, nullptr, st);
 }

@@ -162,6 +162,24 @@ int fe_nuclear_fp64(const void* d_table, const double* d_pts, int n_pts, double*
  * Same values as fastesp.ints.boys (fastesp/ints.py:35-40). */
 int fe_boys_fp64(const double* d_T, int n, int mmax, double* d_F, cudaStream_t stream);
 
+/* fe_esp_fp64 without a caller workspace (no counterpart in the reference).
+ * For callers that cannot allocate device memory -- a host framework that
+ * owns the device-memory budget and lends only input and output buffers, or a
+ * binding of the reference's table-and-points-in / potentials-out interface --
+ * the partial sums live in a file-scope device array of
+ * fe_noalloc_scratch_bytes() (16 MiB) that every GPU loading the library keeps
+ * until the process exits.  Point counts whose scratch would exceed it are
+ * refused with FE_ERR_SIZE (about 10^6 points on a 148-SM B200).  Allocates
+ * nothing: no cudaMalloc, cudaFree or allocating library routine.  The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress)
+ * and should come before any stream capture.  All calls share the array and
+ * every partial sum it holds is rewritten before it is read, so nothing needs
+ * clearing, but calls whose executions overlap on the GPU (other streams, other
+ * host threads) race on it and must be serialised by the caller. */
+int fe_esp_fp64_noalloc(const void* d_table, const double* d_pts, int n_pts, double* d_out,
+                        cudaStream_t stream);
+size_t fe_noalloc_scratch_bytes(void);
+
 /* FMA throughput probe (no counterpart in the reference): ``blocks`` blocks of
  * 256 threads each run ``iters`` iterations of 8 independent FMA chains in FP64
  * (fp64 != 0) or FP32, writing one value per block to d_out.  Timed by the
