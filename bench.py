@@ -173,7 +173,7 @@ def run_ours(args):
     # value: evaluation with the table resident, both precisions
     out = torch.empty(args.points, dtype=torch.float64, device=dev)
     L = _lib.lib()
-    ws = torch.empty(max(256, L.fe_eval_ws_bytes(args.points, 0), L.fe_eval_ws_bytes(args.points, 1)),
+    ws = torch.empty(max(256, tab.ws_bytes(args.points, "fp64"), tab.ws_bytes(args.points, "mixed")),
                      dtype=torch.uint8, device=dev)
     n64 = torch.zeros(1, dtype=torch.int64, device=dev)
 
@@ -283,7 +283,7 @@ def run_ours(args):
     prof = ROOT / "profiles" / f"eval_{'mixed' if prec == 'mixed' else 'f64'}_frag54_30000.json"
     if prof.exists():
         traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
-    launches = 2 if L.fe_eval_ws_bytes(args.points, 1 if prec == "mixed" else 0) > 256 else 1
+    launches = 5 if prec == "mixed" else 3     # evaluator kernel instances + the reduction
     line = {
         "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,

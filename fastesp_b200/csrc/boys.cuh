@@ -8,22 +8,38 @@
 //                            The neglected terms are below 1e-16 relative for
 //                            all orders <= M (thresholds computed in 40-digit
 //                            arithmetic by gen_classes.py).
-//   12 <= T < threshold    : F_0 = sqrt(pi/T)/2 erf(sqrt T) and the upward
-//                            recursion F_(m+1) = ((2m+1) F_m - e^-T)/(2T), which
-//                            loses at most a few percent of an ulp per step at
-//                            T >= 12 for m <= 9.
-//   T < 12                 : F_M from an 8-term Taylor expansion about the
+//   20 <= T < threshold    : F_0 = sqrt(pi/T)/2 - e^-T/(2T) S(1/T) with S the
+//                            asymptotic series of erfc (Abramowitz & Stegun
+//                            7.1.23), S(u) = sum_k (-1)^k (2k-1)!! (u/2)^k,
+//                            12 terms (truncation below 1e-17 of F_0 at T = 20),
+//                            then the upward recursion
+//                            F_(m+1) = ((2m+1) F_m - e^-T)/(2T), which loses at
+//                            most a few percent of an ulp per step at T >= 20.
+//   T < 20                 : F_M from an 8-term Taylor expansion about the
 //                            nearest point of a 1/16 grid (truncation below
 //                            3e-17 relative), then the stable downward recursion
 //                            F_(m-1) = (2T F_m + e^-T)/(2m-1).
 //
-// exp, erf and rsqrt are CUDA's own; the grid values F_n(i/16) are 40-digit
+// exp and rsqrt are CUDA's own; the grid values F_n(i/16) are 40-digit
 // reference values generated into classes_gen.cuh.
 #pragma once
 #include "common.cuh"
 #include "classes_gen.cuh"
 
 #define FE_SQRT_PI_2 0.88622692545275801365   // sqrt(pi)/2
+
+// S(u) = sum_(k=0..11) (-1)^k (2k-1)!! (u/2)^k, Horner form.
+FE_DEV double fe_erfc_asym_series(double u) {
+  const double v = 0.5 * u;
+  double s = -13749310575.0;                       // -(21)!!
+#pragma unroll
+  for (int k = 10; k >= 0; --k) {
+    double c = 1.0;                                // (2k-1)!! with the sign (-1)^k
+    for (int q = 2 * k - 1; q > 1; q -= 2) c *= double(q);
+    s = fma(s, v, (k & 1) ? -c : c);
+  }
+  return s;
+}
 
 template <int M>
 FE_DEV void fe_boys_f64(const double T, double (&F)[M + 1]) {
@@ -38,7 +54,7 @@ FE_DEV void fe_boys_f64(const double T, double (&F)[M + 1]) {
     const double r = rsqrt(T);
     const double h = 0.5 * r * r;
     const double e = exp(-T);
-    F[0] = FE_SQRT_PI_2 * r * erf(T * r);
+    F[0] = fma(-h * e, fe_erfc_asym_series(h + h), FE_SQRT_PI_2 * r);
 #pragma unroll
     for (int m = 0; m < M; ++m) F[m + 1] = fma(double(2 * m + 1), F[m], -e) * h;
   } else {

@@ -11,7 +11,8 @@
 //   p = a + b, P = (aA + bB)/p, K = exp(-ab/p |A-B|^2)       (esp.py:226-230)
 //   E^x_t, E^y_t, E^z_t Hermite coefficients                 (esp.py:108-147)
 //   etab[t] = sum_mu,nu w_mu,nu Ex Ey Ez, w = (D_ij + D_ji) c_a c_b  (esp.py:239-247)
-//   G_k = (2 pi/p)(2p)^m_k sum_t M0[k,t] etab[t]              (esp.py:248-250)
+//   G_k = (2 pi/p)(2p)^m_k sum_t M0[k,t] etab[t]              (esp.py:248-250),
+//         stored at record position fe_gpos_L[k] (the order the kernels read them)
 //   bound = (2p)^-1.5 sum_t |etab_t| M_tx M_ty M_tz (2p)^(|t|/2), reff = 1.6 sqrt((L+2)/p)
 //   screen: rule 0 keeps unless K bound / max(dmin, 0.05) < tol   (table.py:190-194)
 //           rule 1 drops if K bound / max(dmin - reff, 0.05) < tol,
@@ -103,6 +104,14 @@ FE_DEV const float* fe_m0_val() {
   else if constexpr (L == 4) return fe_m0_val_L4; else if constexpr (L == 5) return fe_m0_val_L5;
   else if constexpr (L == 6) return fe_m0_val_L6; else if constexpr (L == 7) return fe_m0_val_L7;
   else return fe_m0_val_L8;
+}
+template <int L>
+FE_DEV const short* fe_gpos() {
+  if constexpr (L == 0) return fe_gpos_L0; else if constexpr (L == 1) return fe_gpos_L1;
+  else if constexpr (L == 2) return fe_gpos_L2; else if constexpr (L == 3) return fe_gpos_L3;
+  else if constexpr (L == 4) return fe_gpos_L4; else if constexpr (L == 5) return fe_gpos_L5;
+  else if constexpr (L == 6) return fe_gpos_L6; else if constexpr (L == 7) return fe_gpos_L7;
+  else return fe_gpos_L8;
 }
 template <int L>
 FE_DEV const signed char* fe_m0_m() {
@@ -233,6 +242,7 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
   const short* rc = fe_m0_col<L>();
   const float* rv = fe_m0_val<L>();
   const signed char* rm = fe_m0_m<L>();
+  const short* gpos = fe_gpos<L>();      // record position of term k (consumption order)
   bool anyg = false;
 #pragma unroll 1
   for (int k = 0; k < NT; ++k) {
@@ -240,7 +250,7 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
     for (int q = rp[k]; q < rp[k + 1]; ++q) s += double(rv[q]) * etab[rc[q]];
     const double g = cf * pw[rm[k]] * s;
     anyg |= (g != 0.0);
-    rec[6 + k] = g;
+    rec[6 + gpos[k]] = g;
   }
   if (a.rule == 1 && !anyg) return;
 

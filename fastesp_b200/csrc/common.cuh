@@ -58,3 +58,4 @@ FE_DEV void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) 
   asm volatile("cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
 }
+

@@ -54,20 +54,29 @@ struct FeBlockWork {
   int hi[FE_NCLASS];
   int ntile[FE_NCLASS];
   int total;
+  int woff[FE_NCLASS];   // first routing-mask word of class L (mixed path)
+  int wtotal;            // routing-mask words per warp
 };
 
-// Thread 0 only.  Classes outside [llo, lhi] get no tiles.
+// Thread 0 only.  Classes outside [llo, lhi] get no tiles.  ``align`` > 1
+// puts every split boundary on a multiple of align pairs (the FP32 kernel uses
+// 32 so that each 32-pair word of its routing mask has a single writer).
 FE_DEV void fe_block_work(const FeTableHdr* hdr, int split, int nsplit, const int* tile_sz,
-                          int llo, int lhi, FeBlockWork& w) {
-  int total = 0;
+                          int llo, int lhi, FeBlockWork& w, int align = 1) {
+  int total = 0, words = 0;
   for (int L = 0; L < FE_NCLASS; ++L) {
     const long long n = (L >= llo && L <= lhi) ? hdr->count[L] : 0;
-    w.lo[L] = int(n * split / nsplit);
-    w.hi[L] = int(n * (split + 1) / nsplit);
-    w.ntile[L] = (w.hi[L] - w.lo[L] + tile_sz[L] - 1) / tile_sz[L];
+    const long long lo = n * split / nsplit / align * align;
+    const long long hi = split + 1 == nsplit ? n : n * (split + 1) / nsplit / align * align;
+    w.lo[L] = int(lo);
+    w.hi[L] = int(hi);
+    w.ntile[L] = int((hi - lo + tile_sz[L] - 1) / tile_sz[L]);
     total += w.ntile[L];
+    w.woff[L] = words;
+    words += (hdr->count[L] + 31) / 32;
   }
   w.total = total;
+  w.wtotal = words;
 }
 
 // Tile i of the block -> (class, first pair, pair count).
@@ -98,9 +107,9 @@ struct FeTilePipe {
   const int64_t* off2 = nullptr;
   int elem2 = 0;
 
-  FE_DEV void start(const FeTableHdr* hdr, int split, int nsplit, int llo, int lhi) {
+  FE_DEV void start(const FeTableHdr* hdr, int split, int nsplit, int llo, int lhi, int align = 1) {
     if (threadIdx.x == 0) {
-      fe_block_work(hdr, split, nsplit, tile_sz, llo, lhi, *w);
+      fe_block_work(hdr, split, nsplit, tile_sz, llo, lhi, *w, align);
       for (int s = 0; s < FE_NSTAGE; ++s) mbar_init(&bar[s], 1);
       mbar_fence_init();
     }
@@ -156,7 +165,7 @@ FE_DEV void fe_tile_f64(const double* __restrict__ rec, int n, const double (&cx
       const double T = pe * fma(x[j], x[j], fma(y[j], y[j], z[j] * z[j]));
       fe_boys_f64<L>(T, F[j]);
     }
-    fe_poly<L, double, NP>(FeCoef<double>{rec + 6}, x, y, z, F, s);
+    fe_poly<L, double, NP>(rec + 6, x, y, z, F, s);
 #pragma unroll
     for (int j = 0; j < NP; ++j) acc[j] = fma(K, s[j], acc[j]);
   }

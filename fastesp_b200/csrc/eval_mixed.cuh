@@ -7,12 +7,13 @@
 //    reference's screening bound, fastesp/esp.py:251-254, evaluated at the
 //    point) bounds sum_k |G_k R^a F_m|; when it reaches ``tau`` for any point
 //    of a warp's point set, that (pair, warp) is evaluated in FP64 instead.
-//    Two kernels share the bit-identical FP32 routing test (fe_route):
-//    fe_eval_f32_kernel evaluates every (pair, warp) the test leaves in FP32
-//    and skips the rest; fe_eval_fix64_kernel evaluates exactly the skipped
-//    ones in FP64.  Neither carries the other's code, so each keeps its
-//    registers, and no state passes between them.  1/|R| comes from the
-//    rsqrt that the FP32 Boys function needs anyway (T^-1/2 = p^-1/2 / |R|).
+//    fe_eval_f32_kernel takes the decision (fe_route), evaluates every
+//    (pair, warp) left in FP32 and records the others as one bit per
+//    (pair, warp) in a routing mask in the workspace; fe_eval_fix64_kernel
+//    walks the set bits and evaluates exactly those pairs in FP64, fetching
+//    only their FP64 records.  Neither kernel carries the other's code, so
+//    each keeps its registers.  1/|R| comes from the rsqrt that the FP32 Boys
+//    function needs anyway (T^-1/2 = p^-1/2 / |R|).
 //  * R = C - P from float hi/lo splits of both coordinates, so R carries about
 //    one float ulp of R itself rather than of |C|.
 //  * accumulation: FP32 contributions into a compensated two-sum pair per
@@ -20,10 +21,13 @@
 //    contributions into an FP64 sum; the splits, the nuclear term and the final
 //    nuclear - electron subtraction are FP64.
 //
-// Grid and pipeline as eval_f64: points in registers (NP per thread), record
-// tiles streamed to shared memory by 1-D TMA bulk copies over an mbarrier ring.
-// Both kernels use the same point blocks (FE_MX_NT threads x FE_MX_NP points),
-// so a warp covers the same points in both and the routing votes agree.
+// Grid and pipeline of the FP32 kernel as eval_f64: points in registers (NP
+// per thread), record tiles streamed to shared memory by 1-D TMA bulk copies
+// over an mbarrier ring.  Both kernels use the same point blocks (FE_MX_NT
+// threads x FE_MX_NP points), so warp g covers the same points in both; its
+// mask row is words [g * wtotal, (g+1) * wtotal), class L from woff[L].  The
+// FP32 kernel's pair splits sit on multiples of 32 pairs, so every mask word
+// has exactly one writer and the mask needs no clearing.
 #pragma once
 #include "eval_f64.cuh"
 
@@ -41,6 +45,8 @@ struct FeMixedArgs {
   int ld;
   float tau;                     // FP64 routing threshold (a.u.)
   unsigned long long* n64;       // optional: count of (pair, warp) FP64 evaluations
+  unsigned* mask;                // routing mask (one bit per pair and warp)
+  long long mask_words;          // its capacity in 32-bit words
 };
 
 __constant__ int fe_c_tile32[FE_NCLASS] = {
@@ -145,64 +151,59 @@ FE_DEV void fe_load_points_split(const double* __restrict__ pts, int npts, int p
   }
 }
 
-// FP32 evaluation of a tile, skipping the (pair, warp) routed to FP64.
+// FP32 evaluation of a tile, recording the (pair, warp) routed to FP64 in the
+// mask instead.  ``first`` is the class-local index of the tile's first pair,
+// ``hi`` the end of this split's range of the class; ``bits`` carries the
+// current mask word across tiles (identical in every lane, lane 0 stores it).
 template <int L, int NP>
-FE_DEV void fe_tile_f32(const float* __restrict__ rec, int n,
+FE_DEV void fe_tile_f32(const float* __restrict__ rec, int first, int n, int hi,
                         const float (&cxh)[NP], const float (&cyh)[NP], const float (&czh)[NP],
                         const float (&cxl)[NP], const float (&cyl)[NP], const float (&czl)[NP],
                         float (&ahi)[NP], float (&alo)[NP], const float* __restrict__ grid,
-                        float tau) {
+                        float tau, unsigned* __restrict__ mw, unsigned& bits) {
   constexpr int S32 = fe_class_rec32[L];
+  const bool lane0 = (threadIdx.x & 31) == 0;
 #pragma unroll 1
   for (int i = 0; i < n; ++i, rec += S32) {
+    const int gi = first + i;
     float x[NP], y[NP], z[NP], r2[NP], ir[NP];
-    if (fe_route<NP>(rec, cxh, cyh, czh, cxl, cyl, czl, x, y, z, r2, ir, tau)) continue;
+    const bool routed = fe_route<NP>(rec, cxh, cyh, czh, cxl, cyl, czl, x, y, z, r2, ir, tau);
+    bits |= unsigned(routed) << (gi & 31);
+    if ((gi & 31) == 31 || gi + 1 == hi) {
+      if (lane0 && mw) mw[gi >> 5] = bits;
+      bits = 0u;
+    }
+    if (routed) continue;
     const float pe = rec[0], rsp = rec[11], K = rec[8];
     float F[NP][L + 1], s[NP];
 #pragma unroll
     for (int j = 0; j < NP; ++j) fe_boys_f32<L>(pe * r2[j], ir[j] * rsp, grid, F[j]);
-    fe_poly<L, float, NP>(FeCoef<float>{rec + 12}, x, y, z, F, s);
+    fe_poly<L, float, NP>(rec + 12, x, y, z, F, s);
 #pragma unroll
     for (int j = 0; j < NP; ++j) fe_two_sum(ahi[j], alo[j], K * s[j]);
   }
 }
 
-// FP64 evaluation of exactly the (pair, warp) the routing test sends to FP64.
-// ``rec`` is the tile's routing (mixed) records, ``rec64`` the same pairs'
-// FP64 records; points are evaluated two at a time for instruction-level
-// parallelism.
+// FP64 evaluation of one routed pair (record ``rec64`` in shared memory) for
+// this thread's points, two at a time for instruction-level parallelism.
 template <int L, int NP>
-FE_DEV void fe_tile_fix64(const float* __restrict__ rec, const double* __restrict__ rec64, int n,
-                          const float (&cxh)[NP], const float (&cyh)[NP], const float (&czh)[NP],
-                          const float (&cxl)[NP], const float (&cyl)[NP], const float (&czl)[NP],
-                          const double (&cx)[NP], const double (&cy)[NP], const double (&cz)[NP],
-                          double (&a64)[NP], float tau, float ox, float oy, float oz, float rad,
-                          unsigned& n64) {
+FE_DEV void fe_pair_fix64(const double* __restrict__ rec64, const double (&cx)[NP],
+                          const double (&cy)[NP], const double (&cz)[NP], double (&a64)[NP]) {
   static_assert(NP % 2 == 0, "points are evaluated in pairs");
-  constexpr int S32 = fe_class_rec32[L];
-  constexpr int S64 = fe_class_rec64[L];
-  const float inv_tau = 1.0f / tau;
+  const double pe = rec64[0], px = rec64[1], py = rec64[2], pz = rec64[3], K = rec64[4];
 #pragma unroll 1
-  for (int i = 0; i < n; ++i, rec += S32, rec64 += S64) {
-    if (fe_out_of_reach(rec, ox, oy, oz, rad, inv_tau)) continue;   // warp-uniform
-    float x[NP], y[NP], z[NP], r2[NP], ir[NP];
-    if (!fe_route<NP>(rec, cxh, cyh, czh, cxl, cyl, czl, x, y, z, r2, ir, tau)) continue;
-    ++n64;
-    const double pe = rec64[0], px = rec64[1], py = rec64[2], pz = rec64[3], K = rec64[4];
-#pragma unroll 1
-    for (int h = 0; h < NP; h += 2) {
-      double xx[2], yy[2], zz[2], F[2][L + 1], s[2];
+  for (int h = 0; h < NP; h += 2) {
+    double xx[2], yy[2], zz[2], F[2][L + 1], s[2];
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        xx[j] = cx[h + j] - px;
-        yy[j] = cy[h + j] - py;
-        zz[j] = cz[h + j] - pz;
-        fe_boys_f64<L>(pe * fma(xx[j], xx[j], fma(yy[j], yy[j], zz[j] * zz[j])), F[j]);
-      }
-      fe_poly<L, double, 2>(FeCoef<double>{rec64 + 6}, xx, yy, zz, F, s);
-#pragma unroll
-      for (int j = 0; j < 2; ++j) a64[h + j] = fma(K, s[j], a64[h + j]);
+    for (int j = 0; j < 2; ++j) {
+      xx[j] = cx[h + j] - px;
+      yy[j] = cy[h + j] - py;
+      zz[j] = cz[h + j] - pz;
+      fe_boys_f64<L>(pe * fma(xx[j], xx[j], fma(yy[j], yy[j], zz[j] * zz[j])), F[j]);
     }
+    fe_poly<L, double, 2>(rec64 + 6, xx, yy, zz, F, s);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) a64[h + j] = fma(K, s[j], a64[h + j]);
   }
 }
 
@@ -236,8 +237,15 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
 #pragma unroll
   for (int j = 0; j < NP; ++j) ahi[j] = alo[j] = 0.0f;
   FeTilePipe pipe{a.table, fe_c_tile32, fe_c_rec32, hdr->off32, 4, fe_smem, full_bar, &w};
-  pipe.start(hdr, blockIdx.y, a.nsplit, LLO, LHI);
+  pipe.start(hdr, blockIdx.y, a.nsplit, LLO, LHI, 32);
   const int total = w.total;
+  const long long warp_g = (long long)blockIdx.x * (NT / 32) + (tid >> 5);
+  unsigned* mrow = a.mask + warp_g * w.wtotal;
+  if ((warp_g + 1) * w.wtotal > a.mask_words) {
+    mrow = nullptr;
+    fe_flag(FE_ST_OVERFLOW);
+  }
+  unsigned bits = 0u;
   for (int i = 0; i < total; ++i) {
     if (!pipe.wait(i)) {
       pipe.abort(i);
@@ -246,7 +254,9 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
     int L, first, n;
     fe_item(w, fe_c_tile32, i, L, first, n);
     const float* rec = reinterpret_cast<const float*>(pipe.stage(i));
-#define FE_CALL32(l) fe_tile_f32<l, NP>(rec, n, cxh, cyh, czh, cxl, cyl, czl, ahi, alo, grid, a.tau)
+    unsigned* mw = mrow ? mrow + w.woff[L] : nullptr;
+#define FE_CALL32(l) fe_tile_f32<l, NP>(rec, first, n, w.hi[L], cxh, cyh, czh, cxl, cyl, czl, \
+                                        ahi, alo, grid, a.tau, mw, bits)
     FE_MX_SWITCH(FE_CALL32)
 #undef FE_CALL32
     pipe.release(i);
@@ -258,18 +268,22 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
   }
 }
 
+// The FP64 part: every warp walks its row of the routing mask over its split's
+// share of the words of each class; for each set bit it copies that pair's
+// FP64 record into a per-warp shared buffer and evaluates it for its points.
+// Pairs are visited in class order, then pair order, so the sum is
+// deterministic.
+#define FE_FIX_BUF 320      // doubles per warp buffer (class-8 record: 300)
+
 template <int MINB, int LLO, int LHI>
 __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_fix64_kernel(const FeMixedArgs a) {
-  constexpr int NP = FE_MX_NP, NT = FE_MX_NT;
-  extern __shared__ __align__(128) unsigned char fe_smem[];
-  __shared__ uint64_t full_bar[FE_NSTAGE];
+  constexpr int NP = FE_MX_NP, NT = FE_MX_NT, NW = FE_MX_NT / 32;
+  __shared__ __align__(16) double buf[NW][FE_FIX_BUF];
   __shared__ FeBlockWork w;
   const FeTableHdr* hdr = reinterpret_cast<const FeTableHdr*>(a.table);
-  const int tid = threadIdx.x;
-  float cxh[NP], cyh[NP], czh[NP], cxl[NP], cyl[NP], czl[NP];
+  const int tid = threadIdx.x, lane = tid & 31, wi = tid >> 5;
   double cx[NP], cy[NP], cz[NP], a64[NP];
   const int p0 = int(blockIdx.x) * (NT * NP) + tid;
-  fe_load_points_split<NP>(a.pts, a.npts, p0, NT, cxh, cyh, czh, cxl, cyl, czl);
 #pragma unroll
   for (int j = 0; j < NP; ++j) {
     const int q = min(p0 + j * NT, a.npts - 1);
@@ -278,29 +292,47 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_fix64_kernel(const FeM
     cz[j] = a.pts[3 * q + 2];
     a64[j] = 0.0;
   }
-  float ox, oy, oz, rad;
-  fe_warp_sphere<NP>(cxh, cyh, czh, ox, oy, oz, rad);
-  unsigned n64 = 0;
-  FeTilePipe pipe{a.table, fe_c_tilefix, fe_c_rec32, hdr->off32, 4, fe_smem, full_bar, &w,
-                  fe_c_rec64, hdr->off64, 8};
-  pipe.start(hdr, blockIdx.y, a.nsplit, LLO, LHI);
-  const int total = w.total;
-  for (int i = 0; i < total; ++i) {
-    if (!pipe.wait(i)) {
-      pipe.abort(i);
-      return;
-    }
-    int L, first, n;
-    fe_item(w, fe_c_tilefix, i, L, first, n);
-    const float* rec = reinterpret_cast<const float*>(pipe.stage(i));
-    const double* rec64 = reinterpret_cast<const double*>(pipe.stage(i) + size_t(n) * fe_c_rec32[L] * 4);
-#define FE_CALL64(l) fe_tile_fix64<l, NP>(rec, rec64, n, cxh, cyh, czh, cxl, cyl, czl, cx, cy, cz, \
-                                          a64, a.tau, ox, oy, oz, rad, n64)
-    FE_MX_SWITCH(FE_CALL64)
-#undef FE_CALL64
-    pipe.release(i);
+  if (tid == 0) {
+    const int one[FE_NCLASS] = {1, 1, 1, 1, 1, 1, 1, 1, 1};
+    fe_block_work(hdr, 0, 1, one, 0, FE_NCLASS - 1, w);    // word offsets only
   }
-  if (a.n64 && (tid & 31) == 0) atomicAdd(a.n64, (unsigned long long)n64);
+  __syncthreads();
+  const long long warp_g = (long long)blockIdx.x * NW + wi;
+  unsigned n64 = 0;
+  if ((warp_g + 1) * w.wtotal <= a.mask_words) {
+    const unsigned* mrow = a.mask + warp_g * w.wtotal;
+    for (int L = LLO; L <= LHI; ++L) {
+      const int nw = (hdr->count[L] + 31) / 32;
+      const int w0 = int((long long)nw * blockIdx.y / a.nsplit);
+      const int w1 = int((long long)nw * (blockIdx.y + 1) / a.nsplit);
+      const int S64 = fe_c_rec64[L];
+      const double* base = reinterpret_cast<const double*>(a.table + hdr->off64[L]);
+      for (int c = w0; c < w1; c += 32) {
+        const unsigned word = c + lane < w1 ? mrow[w.woff[L] + c + lane] : 0u;
+        unsigned live = __ballot_sync(0xffffffffu, word != 0u);
+        while (live) {
+          const int src = __ffs(live) - 1;
+          live &= live - 1;
+          unsigned bitsw = __shfl_sync(0xffffffffu, word, src);
+          while (bitsw) {
+            const int b = __ffs(bitsw) - 1;
+            bitsw &= bitsw - 1;
+            const double* r = base + size_t((c + src) * 32 + b) * S64;
+            __syncwarp();
+            for (int k = lane; k < S64; k += 32) buf[wi][k] = __ldg(r + k);
+            __syncwarp();
+            ++n64;
+#define FE_CALLP(l) fe_pair_fix64<l, NP>(buf[wi], cx, cy, cz, a64)
+            FE_MX_SWITCH(FE_CALLP)
+#undef FE_CALLP
+          }
+        }
+      }
+    }
+  } else {
+    fe_flag(FE_ST_OVERFLOW);
+  }
+  if (a.n64 && lane == 0) atomicAdd(a.n64, (unsigned long long)n64);
 #pragma unroll
   for (int j = 0; j < NP; ++j) {
     const int p = p0 + j * NT;

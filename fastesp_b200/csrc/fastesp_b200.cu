@@ -511,10 +511,19 @@ int fe_table_info_get(const void* d_table, fe_table_info* info, cudaStream_t st)
   return FE_OK;
 }
 
-size_t fe_eval_ws_bytes(int n_pts, int mode) {
+size_t fe_eval_ws_bytes(int n_pts) {
   if (n_pts <= 0) return 256;
-  const EvalGeom g = eval_geom(n_pts, mode == 1 ? 1 : 0);
+  const EvalGeom g = eval_geom(n_pts, 0);
   return align256(g.ws_rows() * g.ld * sizeof(double));
+}
+
+size_t fe_eval_ws_bytes_mixed(int n_pts, const int* cap) {
+  if (n_pts <= 0) return 256;
+  const EvalGeom g = eval_geom(n_pts, 1);
+  long long words = 0;
+  for (int L = 0; L < FE_NCLASS; ++L) words += cap ? (std::max(cap[L], 0) + 31) / 32 : 0;
+  const long long warps = (long long)g.nblk_x * (FE_MX_NT / 32);
+  return align256(g.ws_rows() * g.ld * sizeof(double)) + align256(size_t(warps * words) * 4);
 }
 
 }  // extern "C"
@@ -528,9 +537,9 @@ int eval_launch(const char* who, const void* d_table, const double* d_pts, int n
   if (n_pts == 0) return FE_OK;
   if (!d_table || !d_pts || !d_out) return fail(FE_ERR_ARG, "%s: null argument", who);
   const EvalGeom g = eval_geom(n_pts, prec);
-  if (!d_ws || ws_bytes < g.ws_rows() * g.ld * sizeof(double))
-    return fail(FE_ERR_SIZE, "%s: workspace too small (need %zu bytes)", who,
-                fe_eval_ws_bytes(n_pts, prec));
+  const size_t rows_bytes = align256(g.ws_rows() * g.ld * sizeof(double));
+  if (!d_ws || ws_bytes < rows_bytes)
+    return fail(FE_ERR_SIZE, "%s: workspace too small (need at least %zu bytes)", who, rows_bytes);
   const int smem = FE_NSTAGE * FE_STAGE_BYTES;
   double* rows = static_cast<double*>(d_ws);
   auto next_rows = [&](int k) {
@@ -557,6 +566,9 @@ int eval_launch(const char* who, const void* d_table, const double* d_pts, int n
     FE_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     k1<<<dim3(g.nblk_x, g.split[1]), kEvalThreads, smem, st>>>(a);
   } else {
+    if (ws_bytes - rows_bytes < 4)
+      return fail(FE_ERR_SIZE, "%s: workspace has no room for the routing mask (size it with "
+                  "fe_eval_ws_bytes_mixed)", who);
     FeMixedArgs a{};
     a.table = tb;
     a.pts = d_pts;
@@ -564,6 +576,8 @@ int eval_launch(const char* who, const void* d_table, const double* d_pts, int n
     a.ld = g.ld;
     a.tau = float(tau);
     a.n64 = d_n64;
+    a.mask = reinterpret_cast<unsigned*>(static_cast<unsigned char*>(d_ws) + rows_bytes);
+    a.mask_words = static_cast<long long>((ws_bytes - rows_bytes) / 4);
     auto f0 = fe_eval_f32_kernel<kMinB32, 0, FE_LSPLIT>;
     auto f1 = fe_eval_f32_kernel<1, FE_LSPLIT + 1, FE_NCLASS - 1>;
     auto x0 = fe_eval_fix64_kernel<kMinBFix, 0, FE_LSPLIT>;
@@ -572,9 +586,10 @@ int eval_launch(const char* who, const void* d_table, const double* d_pts, int n
     for (int k = 0; k < 4; ++k) {
       a.nsplit = g.split[k];
       a.partial = next_rows(k);
-      FE_CUDA(cudaFuncSetAttribute(ks[k], cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      const int dyn = k < 2 ? smem : 0;      // the FP64 part uses static buffers only
+      if (dyn) FE_CUDA(cudaFuncSetAttribute(ks[k], cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
       void* args[] = {&a};
-      FE_CUDA(cudaLaunchKernel(ks[k], dim3(g.nblk_x, g.split[k]), dim3(FE_MX_NT), args, smem, st));
+      FE_CUDA(cudaLaunchKernel(ks[k], dim3(g.nblk_x, g.split[k]), dim3(FE_MX_NT), args, dyn, st));
     }
   }
   FE_CUDA(cudaGetLastError());
@@ -737,7 +752,7 @@ extern "C" int fe_esp_fp64_noalloc(const void* d_table, const double* d_pts, int
   if (n_pts < 0) return fail(FE_ERR_ARG, "fe_esp_fp64_noalloc: n_pts < 0");
   if (n_pts == 0) return FE_OK;
   if (!d_table || !d_pts || !d_out) return fail(FE_ERR_ARG, "fe_esp_fp64_noalloc: null argument");
-  const size_t need = fe_eval_ws_bytes(n_pts, 0);
+  const size_t need = fe_eval_ws_bytes(n_pts);
   if (need > FE_NOALLOC_SCRATCH_BYTES)
     return fail(FE_ERR_SIZE,
                 "fe_esp_fp64_noalloc: %d points need %zu bytes of scratch, more than the "

@@ -18,6 +18,7 @@ For every angular class L = la + lb (0..8) this emits
 from __future__ import annotations
 
 import sys
+from functools import lru_cache
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
@@ -29,7 +30,7 @@ LMAX = 2 * H.LMAX_SHELL        # largest class
 MMAX = LMAX + 1                # largest Boys order needed (adjoint needs L+1)
 TAYLOR_K = 8                   # Taylor terms of the tabulated branch
 GRID_H = 1.0 / 16.0            # grid spacing of the tabulated branch
-GRID_TMAX = 12.0               # tabulated branch covers 0 <= T < GRID_TMAX
+GRID_TMAX = 20.0               # tabulated branch covers 0 <= T < GRID_TMAX
 NTAB = MMAX + TAYLOR_K         # orders stored per grid row
 TAYLOR_K32 = 6                 # FP32 grid: Taylor terms
 GRID_H32 = 1.0 / 4.0           # FP32 grid spacing (truncation < 6e-9 relative)
@@ -87,30 +88,63 @@ class Emitter:
                 self.nops += 1
 
 
-def poly_m_major(L):
+class CoefLoader:
+    """Hands out coefficient expressions in first-use (consumption) order.
+
+    The record stores class-L coefficients in this order, so the generated
+    code reads them front to back: ``vec`` > 0 emits one 16-byte vector load
+    per ``vec`` consecutive coefficients (float4 / double2), 0 scalar loads.
+    """
+
+    def __init__(self, em, order=None, vec=0, vtype=""):
+        self.em = em
+        self.pos = {} if order is None else {k: i for i, k in enumerate(order)}
+        self.fixed = order is not None
+        self.vec = vec
+        self.vtype = vtype
+        self.loaded = set()
+
+    def expr(self, k):
+        if k not in self.pos:
+            assert not self.fixed
+            self.pos[k] = len(self.pos)
+        p = self.pos[k]
+        if not self.vec:
+            return f"g[{p}]"
+        c, lane = divmod(p, self.vec)
+        if c not in self.loaded:
+            self.loaded.add(c)
+            self.em.w(f"const {self.vtype} gv{c} = *reinterpret_cast<const {self.vtype}*>(g + {c * self.vec});")
+        return f"gv{c}.{'xyzw'[lane]}"
+
+    def order(self):
+        return [k for k, _ in sorted(self.pos.items(), key=lambda kv: kv[1])]
+
+
+def poly_m_major(L, order=None, vec=0, vtype=""):
     keys, _ = H.class_terms(L)
     em = Emitter()
+    ld = CoefLoader(em, order, vec, vtype)
     by_m = {}
     for k, (ax, ay, az, m) in enumerate(keys):
         by_m.setdefault(m, {})[(ax, ay, az)] = k
     acc = ("ha", "hb", "hc")
     first = True
     for m in sorted(by_m):
-        def coef(k):
-            return f"const Real g{k} = g({k});", f"g{k}"
-        em.horner(by_m[m], 0, acc, coef)
+        em.horner(by_m[m], 0, acc, lambda k: (None, ld.expr(k)))
         if first:
             em.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) s[j] = F[j][{m}] * ha[j];")
             first = False
         else:
             em.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) s[j] = fe_fma(F[j][{m}], ha[j], s[j]);")
         em.nops += 1
-    return em
+    return em, ld
 
 
-def poly_alpha_major(L):
+def poly_alpha_major(L, order=None, vec=0, vtype=""):
     keys, _ = H.class_terms(L)
     em = Emitter()
+    ld = CoefLoader(em, order, vec, vtype)
     by_a = {}
     for k, (ax, ay, az, m) in enumerate(keys):
         by_a.setdefault((ax, ay, az), []).append((k, m))
@@ -118,37 +152,53 @@ def poly_alpha_major(L):
 
     def coef(a):
         ks = by_a[a]
-        lines = []
         k0, m0 = ks[0]
-        lines.append(f"const Real g{k0} = g({k0}); "
-                     f"FE_UNROLL for (int j = 0; j < NP; ++j) hd[j] = g{k0} * F[j][{m0}];")
+        em.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) hd[j] = {ld.expr(k0)} * F[j][{m0}];")
         em.nops += 1
         for k, m in ks[1:]:
-            lines.append(f"const Real g{k} = g({k}); "
-                         f"FE_UNROLL for (int j = 0; j < NP; ++j) hd[j] = fe_fma(g{k}, F[j][{m}], hd[j]);")
+            em.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) hd[j] = fe_fma({ld.expr(k)}, F[j][{m}], hd[j]);")
             em.nops += 1
-        return " ".join(lines), "hd[j]"
+        return None, "hd[j]"
 
-    alpha_terms = {a: a for a in by_a}
-    em.horner(alpha_terms, 0, acc, coef)
+    em.horner({a: a for a in by_a}, 0, acc, coef)
     em.w("FE_UNROLL for (int j = 0; j < NP; ++j) s[j] = ha[j];")
-    return em
+    return em, ld
 
 
-def poly_function(L):
-    a = poly_m_major(L)
-    b = poly_alpha_major(L)
-    em, tag = (a, "m-major") if a.nops <= b.nops else (b, "alpha-major")
-    out = [f"// class L={L}: {H.n_terms(L)} terms, {em.nops} fused ops per point ({tag})",
-           "template <typename Real, int NP, typename GL>",
-           f"__device__ __forceinline__ void fe_poly_L{L}(const GL& g,",
-           "    const Real (&x)[NP], const Real (&y)[NP], const Real (&z)[NP],",
-           f"    const Real (&F)[NP][{L + 1}], Real (&s)[NP]) {{",
-           "  Real ha[NP], hb[NP], hc[NP], hd[NP];",
-           "  (void)hb; (void)hc; (void)hd;"]
-    out += em.lines
-    out.append("}")
-    return out, em.nops
+def poly_variant(L):
+    """(builder, tag) of the cheaper of the two nested-Horner orders for class L."""
+    a, _ = poly_m_major(L)
+    b, _ = poly_alpha_major(L)
+    return (poly_m_major, "m-major", a.nops) if a.nops <= b.nops else \
+        (poly_alpha_major, "alpha-major", b.nops)
+
+
+@lru_cache(maxsize=None)
+def consumption_order(L):
+    """Term indices k in the order the class-L code reads them = record order."""
+    build, _, _ = poly_variant(L)
+    return build(L)[1].order()
+
+
+def poly_functions(L):
+    build, tag, nops = poly_variant(L)
+    order = consumption_order(L)
+    out = []
+    for real, vtype, vec, suffix in (("float", "float4", 4, "32"), ("double", "double2", 2, "64")):
+        em, _ = build(L, order, vec, vtype)
+        out += [f"// class L={L}: {H.n_terms(L)} terms, {nops} fused ops per point ({tag}),",
+                f"// coefficients g[0..{H.n_terms(L)}) in consumption order, 16-byte aligned",
+                "template <int NP>",
+                f"__device__ __forceinline__ void fe_poly{suffix}_L{L}(const {real}* __restrict__ g,",
+                f"    const {real} (&x)[NP], const {real} (&y)[NP], const {real} (&z)[NP],",
+                f"    const {real} (&F)[NP][{L + 1}], {real} (&s)[NP]) {{",
+                "  using Real = " + real + ";",
+                "  Real ha[NP], hb[NP], hc[NP], hd[NP];",
+                "  (void)hb; (void)hc; (void)hd;"]
+        out += em.lines
+        out.append("}")
+        out.append("")
+    return out, nops
 
 
 def grad_function(L):
@@ -156,26 +206,23 @@ def grad_function(L):
 
     Written as s, u = sum_k G_k R^a F_(m+1) and the three partial derivatives
     of the monomials, each again in Horner form over exponents; F carries
-    orders 0..L+1.
+    orders 0..L+1.  Coefficients are read from the record's consumption order.
     """
     keys, _ = H.class_terms(L)
+    pos = {k: i for i, k in enumerate(consumption_order(L))}
     em = Emitter()
     acc = ("ha", "hb", "hc")
-    outs = []
-    # value s and u: same monomials, Boys order m and m+1
     for name, shift in (("s", 0), ("u", 1)):
         by_m = {}
         for k, (ax, ay, az, m) in enumerate(keys):
             by_m.setdefault(m + shift, {})[(ax, ay, az)] = k
         first = True
         for m in sorted(by_m):
-            em.horner(by_m[m], 0, acc, lambda k: (f"const Real g{k}_{name}{m} = g({k});",
-                                                 f"g{k}_{name}{m}"))
+            em.horner(by_m[m], 0, acc, lambda k: (None, f"g[{pos[k]}]"))
             op = (f"{name}[j] = F[j][{m}] * ha[j];" if first else
                   f"{name}[j] = fe_fma(F[j][{m}], ha[j], {name}[j]);")
             em.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) {op}")
             first = False
-    # derivative of the monomials: d/dR_c R^a = a_c R^(a - e_c)
     for c, cname in enumerate(("dx", "dy", "dz")):
         by_m = {}
         for k, key in enumerate(keys):
@@ -189,9 +236,7 @@ def grad_function(L):
         first = True
         for m in sorted(by_m):
             em.horner(by_m[m], 0, acc,
-                      lambda kf, c=c, m=m: (f"const Real g{kf[0]}_d{c}{m} = "
-                                            f"Real({kf[1]}) * g({kf[0]});",
-                                            f"g{kf[0]}_d{c}{m}"))
+                      lambda kf: (None, f"(Real({kf[1]}) * g[{pos[kf[0]]}])"))
             op = (f"{cname}[j] = F[j][{m}] * ha[j];" if first else
                   f"{cname}[j] = fe_fma(F[j][{m}], ha[j], {cname}[j]);")
             em.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) {op}")
@@ -199,8 +244,8 @@ def grad_function(L):
         if first:
             em.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) {cname}[j] = Real(0);")
     out = [f"// class L={L}: value, F_(m+1) companion sum and monomial derivatives",
-           "template <typename Real, int NP, typename GL>",
-           f"__device__ __forceinline__ void fe_grad_L{L}(const GL& g,",
+           "template <typename Real, int NP>",
+           f"__device__ __forceinline__ void fe_grad_L{L}(const Real* __restrict__ g,",
            "    const Real (&x)[NP], const Real (&y)[NP], const Real (&z)[NP],",
            f"    const Real (&F)[NP][{L + 2}], Real (&s)[NP], Real (&u)[NP],",
            "    Real (&dx)[NP], Real (&dy)[NP], Real (&dz)[NP]) {",
@@ -346,10 +391,15 @@ def main() -> int:
     # polynomial evaluators
     nops = []
     for L in range(LMAX + 1):
-        lines, n = poly_function(L)
+        lines, n = poly_functions(L)
         nops.append(n)
         out += lines
-        out.append("")
+    # record position of every term (the builder writes G_k at fe_gpos_L[k])
+    for L in range(LMAX + 1):
+        pos = {k: i for i, k in enumerate(consumption_order(L))}
+        out.append(f"__constant__ short fe_gpos_L{L}[{H.n_terms(L)}] = {{"
+                   + ", ".join(str(pos[k]) for k in range(H.n_terms(L))) + "};")
+    out.append("")
     out.append("static constexpr int fe_class_polyops[FE_NCLASS] = {"
                + ", ".join(map(str, nops)) + "};")
     out.append("")
@@ -357,37 +407,27 @@ def main() -> int:
         out += grad_function(L)
         out.append("")
     # compile-time dispatch on the class
-    out.append("// g(k): coefficient k of the class's term list (a plain array or a split record)")
-    out.append("template <typename Real>")
-    out.append("struct FeCoef {")
-    out.append("  const Real* __restrict__ p;")
-    out.append("  __device__ __forceinline__ Real operator()(int k) const { return p[k]; }")
-    out.append("};")
-    out.append("struct FeCoefSplit {   // double from a float hi/lo pair")
-    out.append("  const float* __restrict__ hi;")
-    out.append("  const float* __restrict__ lo;")
-    out.append("  __device__ __forceinline__ double operator()(int k) const {")
-    out.append("    return double(hi[k]) + double(lo[k]);")
-    out.append("  }")
-    out.append("};")
-    out.append("")
-    out.append("template <int L, typename Real, int NP, typename GL>")
-    out.append("__device__ __forceinline__ void fe_poly(const GL& g,")
+    out.append("// s = sum_k G_k R^a F_m for class L; g: the record's coefficients (consumption order)")
+    out.append("template <int L, typename Real, int NP>")
+    out.append("__device__ __forceinline__ void fe_poly(const Real* __restrict__ g,")
     out.append("    const Real (&x)[NP], const Real (&y)[NP], const Real (&z)[NP],")
     out.append("    const Real (&F)[NP][L + 1], Real (&s)[NP]) {")
     for L in range(LMAX + 1):
         kw = "if" if L == 0 else "else if"
-        out.append(f"  {kw} constexpr (L == {L}) fe_poly_L{L}<Real, NP, GL>(g, x, y, z, F, s);")
+        out.append(f"  {kw} constexpr (L == {L}) {{")
+        out.append(f"    if constexpr (sizeof(Real) == 4) fe_poly32_L{L}<NP>(g, x, y, z, F, s);")
+        out.append(f"    else fe_poly64_L{L}<NP>(g, x, y, z, F, s);")
+        out.append("  }")
     out.append("}")
     out.append("")
-    out.append("template <int L, typename Real, int NP, typename GL>")
-    out.append("__device__ __forceinline__ void fe_grad(const GL& g,")
+    out.append("template <int L, typename Real, int NP>")
+    out.append("__device__ __forceinline__ void fe_grad(const Real* __restrict__ g,")
     out.append("    const Real (&x)[NP], const Real (&y)[NP], const Real (&z)[NP],")
     out.append("    const Real (&F)[NP][L + 2], Real (&s)[NP], Real (&u)[NP],")
     out.append("    Real (&dx)[NP], Real (&dy)[NP], Real (&dz)[NP]) {")
     for L in range(LMAX + 1):
         kw = "if" if L == 0 else "else if"
-        out.append(f"  {kw} constexpr (L == {L}) fe_grad_L{L}<Real, NP, GL>(g, x, y, z, F, s, u, dx, dy, dz);")
+        out.append(f"  {kw} constexpr (L == {L}) fe_grad_L{L}<Real, NP>(g, x, y, z, F, s, u, dx, dy, dz);")
     out.append("}")
     out.append("")
     out.append("__constant__ int fe_c_rec64[FE_NCLASS] = {"

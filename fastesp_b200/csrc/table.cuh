@@ -7,7 +7,8 @@
 //
 // Pairs are grouped by angular class L = la + lb.  A class-L FP64 record is
 // fe_class_rec64[L] doubles: [p, Px, Py, Pz, K, K*bound, G_0 .. G_(nt-1), pad]
-// (K*bound is the screening bound's numerator, +inf when unknown), so the
+// (K*bound is the screening bound's numerator, +inf when unknown; the G_k are
+// stored in the order the class's generated code reads them, fe_gpos_L), so the
 // records of a tile are one contiguous, 16-byte-aligned run that a single
 // bulk copy moves into shared memory.  Within a class, pairs keep the order of
 // the reference builder: shell pairs (si <= sj) in shell order, then

@@ -65,6 +65,15 @@ def _is_torch(a) -> bool:
         return False
 
 
+def _gpos(L: int) -> np.ndarray:
+    """Record position of every class-L term (the order the kernels read them)."""
+    from .csrc.gen_classes import consumption_order
+    order = consumption_order(L)
+    pos = np.empty(len(order), np.int64)
+    pos[np.array(order)] = np.arange(len(order))
+    return pos
+
+
 def _empty_bytes(n, device):
     torch = _torch()
     return torch.empty(max(int(n), 256), dtype=torch.uint8, device=device)
@@ -253,16 +262,20 @@ class PairTable:
             _lib.check(L.fe_nuclear_fp64(_lib.ptr(self._buf), _lib.ptr(d), n, _lib.ptr(out),
                                          None, 0, s))
         elif precision == "fp64":
-            ws = _empty_bytes(L.fe_eval_ws_bytes(n, 0), self.device)
+            ws = _empty_bytes(_lib.ws_bytes(n, "fp64"), self.device)
             fn = L.fe_esp_fp64 if mode == 0 else L.fe_electron_fp64
             _lib.check(fn(_lib.ptr(self._buf), _lib.ptr(d), n, _lib.ptr(out), _lib.ptr(ws),
                           ws.numel(), s))
         else:
-            ws = _empty_bytes(L.fe_eval_ws_bytes(n, 1), self.device)
+            ws = _empty_bytes(self.ws_bytes(n, "mixed"), self.device)
             fn = L.fe_esp_mixed if mode == 0 else L.fe_electron_mixed
             _lib.check(fn(_lib.ptr(self._buf), _lib.ptr(d), n, _lib.ptr(out), _lib.ptr(ws),
                           ws.numel(), float(tau), _lib.ptr(n64), s))
         return out.cpu().numpy() if as_numpy else out
+
+    def ws_bytes(self, n_points: int, precision: str = "fp64") -> int:
+        """Workspace bytes of an evaluation of ``n_points`` points with this table."""
+        return _lib.ws_bytes(n_points, precision, self.info_caps())
 
     def esp_stats(self, points=None, tau: float = 0.0):
         """Mixed-precision ESP and the number of (pair, warp) evaluations routed to FP64."""
@@ -272,6 +285,12 @@ class PairTable:
         return v, int(n64.item())
 
     # -- export / import (pairs.bin) -----------------------------------
+    def coefficients(self, L: int) -> np.ndarray:
+        """(count, nt) G coefficients of class L in the reference's term order."""
+        r = self.records(L)
+        pos = _gpos(L)
+        return r[:, 6 + pos]
+
     def records(self, L: int) -> np.ndarray:
         """(count, rec64) FP64 records of class L copied to the host."""
         n = self.counts[L]
@@ -320,7 +339,7 @@ class PairTable:
             pp["mo_axis"].append(np.tile(axis, n))
             pp["tm_aidx"].append(np.tile(aidx, n))
             pp["tm_m"].append(np.tile(H.term_m(L), n))
-            pp["tm_g"].append(r[:, 6:6 + nt].ravel())
+            pp["tm_g"].append(r[:, 6 + _gpos(L)].ravel())
             toff += nt * n
             moff += nm * n
         out = {}
@@ -403,7 +422,7 @@ class PairTable:
                 rec[:, 3] = a["pp_cz"][sel]
                 rec[:, 4] = a["pp_K"][sel]
                 rec[:, 5] = np.inf          # no screening bound in pairs.bin
-                rec[:, 6:6 + ntL] = a["tm_g"][toff]
+                rec[:, 6 + _gpos(L)] = a["tm_g"][toff]
             recs.append(rec)
         L_ = _lib.lib()
         cap = (C.c_int * NCLASS)(*counts)

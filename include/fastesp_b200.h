@@ -123,9 +123,15 @@ int fe_table_make_f32(void* d_table, cudaStream_t stream);
 /* Copy the table header to the host (synchronises ``stream``). */
 int fe_table_info_get(const void* d_table, fe_table_info* info, cudaStream_t stream);
 
-/* Workspace bytes of an evaluation of n_pts points (mode 0 FP64, 1 mixed);
- * holds the per-split partial sums of the pair-split reduction. */
-size_t fe_eval_ws_bytes(int n_pts, int mode);
+/* Workspace bytes of an FP64 evaluation of n_pts points: the per-split
+ * partial sums of the pair-split reduction. */
+size_t fe_eval_ws_bytes(int n_pts);
+
+/* Workspace bytes of a mixed-precision evaluation of n_pts points of a table
+ * holding at most cap[L] pairs of class L (fe_sizes.cap of its plan, or the
+ * counts of an imported table): partial sums plus the FP64 routing mask (one
+ * bit per pair and warp of points). */
+size_t fe_eval_ws_bytes_mixed(int n_pts, const int* cap);
 
 /* V(C) = sum_A Z_A/|C-R_A| - sum_pairs K sum_k G_k R^alpha F_m(p R^2), all FP64,
  * for the (n_pts, 3) points ``d_pts`` into ``d_out`` (n_pts,).  Replaces

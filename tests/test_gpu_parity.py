@@ -89,7 +89,7 @@ def test_build_matches_reference_table(tag, request):
         np.testing.assert_allclose(rec[:, 4], g["tab_pp_K"][rows], rtol=1e-13)
         nt = H.n_terms(L)
         off = g["tab_pp_off"][rows][:, None] + np.arange(nt)[None, :]
-        np.testing.assert_allclose(rec[:, 6:6 + nt], g["tab_tm_g"][off], rtol=0, atol=1e-13 * gmax)
+        np.testing.assert_allclose(tab.coefficients(L), g["tab_tm_g"][off], rtol=0, atol=1e-13 * gmax)
 
 
 @pytest.mark.parametrize("tag", ["small", "tz6"])
@@ -347,7 +347,7 @@ def test_every_workspace_row_is_written(frag54, npts, prec):
     tab = build_table(wfn, basis, P, pts, tol=1e-12)
     L = _lib.lib()
     mode = 0 if prec == "fp64" else 1
-    nb = L.fe_eval_ws_bytes(npts, mode)
+    nb = tab.ws_bytes(npts, prec)
     ws = torch.full((nb // 8,), float("nan"), dtype=torch.float64, device="cuda")
     out = torch.full((npts,), float("nan"), dtype=torch.float64, device="cuda")
     if prec == "fp64":

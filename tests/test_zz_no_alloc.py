@@ -31,7 +31,7 @@ def test_noalloc_matches_workspace_entry_point(npts):
     L = _lib.lib()
     pd = torch.as_tensor(pts, device="cuda")
     ref = torch.empty(npts, dtype=torch.float64, device="cuda")
-    ws = torch.empty(L.fe_eval_ws_bytes(npts, 0), dtype=torch.uint8, device="cuda")
+    ws = torch.empty(L.fe_eval_ws_bytes(npts), dtype=torch.uint8, device="cuda")
     _lib.check(L.fe_esp_fp64(_lib.ptr(tab._buf), _lib.ptr(pd), npts, _lib.ptr(ref),
                              _lib.ptr(ws), ws.numel(), _lib.stream_ptr()))
     want = ref.cpu().numpy()
@@ -50,7 +50,7 @@ def test_noalloc_refuses_oversized_point_counts():
     L = _lib.lib()
     cap = L.fe_noalloc_scratch_bytes()
     n = 1
-    while L.fe_eval_ws_bytes(n, 0) <= cap:
+    while L.fe_eval_ws_bytes(n) <= cap:
         n *= 2
     wfn, basis, P, pts = synth.load_workload("small", 10, seed=0)
     tab = build_table(wfn, basis, P, pts, tol=1e-12)
