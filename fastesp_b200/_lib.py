@@ -75,6 +75,10 @@ _SIGS = {
     "fe_peak_run": (C.c_int, [C.c_int, C.c_longlong, C.c_int, _P, _P]),
     "fe_esp_fp64_noalloc": (C.c_int, [_P, _P, C.c_int, _P, _P]),
     "fe_noalloc_scratch_bytes": (C.c_size_t, []),
+    "fe_field_ws_bytes": (C.c_size_t, [C.c_int]),
+    "fe_esp_field_fp64": (C.c_int, [_P, _P, C.c_int, _P, _P, _P, _P, C.c_size_t, _P]),
+    "fe_adjoint_ws_bytes": (C.c_size_t, [_P, C.c_int]),
+    "fe_esp_adjoint": (C.c_int, [_P, _P, _P, _P, C.c_int, _P, _P, _P, _P, C.c_size_t, _P]),
 }
 
 _lock = threading.Lock()

@@ -56,6 +56,7 @@ struct FeBuildArgs {
   const long long* stage_off;
   int* keep;                     // per global slot
   double* srule;                 // per global slot: K (pi/p)^1.5 etab[0]
+  int* swork;                    // per global slot: its work item
 };
 
 __constant__ signed char fe_cart[5][15][3] = {
@@ -167,6 +168,7 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
   const long long slot = a.class_slot0[L] + tk.slot0 + ii * B.nprim + jj;
   a.keep[slot] = 0;
   a.srule[slot] = 0.0;
+  a.swork[slot] = w;
 
   // density block of the shell pair (both orderings for si != sj)
   double W[NA * NB];
@@ -317,12 +319,14 @@ __global__ void __launch_bounds__(FE_BUILD_THREADS) fe_build_kernel(const FeBuil
   }
 }
 
-// Move kept staging records of every class, in slot order, into the table.
+// Move kept staging records of every class, in slot order, into the table,
+// and record each one's work item in the table's source section.
 // ``pos`` is the exclusive scan of ``keep`` over all global slots.
 __global__ void fe_scatter_kernel(const double* __restrict__ stage, const long long* stage_off,
                                   const long long* class_slot0, int nclass,
                                   const int* __restrict__ keep, const int* __restrict__ pos,
-                                  long long nslot, unsigned char* table) {
+                                  const int* __restrict__ swork, long long nslot,
+                                  unsigned char* table) {
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s >= nslot || !keep[s]) return;
   int L = 0;
@@ -334,6 +338,9 @@ __global__ void fe_scatter_kernel(const double* __restrict__ stage, const long l
   const double* src = stage + stage_off[L] + (s - class_slot0[L]) * R;
   double* out = reinterpret_cast<double*>(table + hdr->off64[L]) + size_t(dst) * R;
   for (int k = 0; k < R; ++k) out[k] = src[k];
+  long long base = 0;
+  for (int l = 0; l < L; ++l) base += hdr->cap[l];
+  reinterpret_cast<int*>(table + hdr->off_src)[base + dst] = swork[s];
 }
 
 // Per-class kept counts and the sum rule.  One block of 1024 threads: each
@@ -357,7 +364,10 @@ __global__ void __launch_bounds__(1024) fe_finalize_kernel(
     if (t < h) red[t] += red[t + h];
     __syncthreads();
   }
-  if (t == 0) hdr->sum_rule = red[0];
+  if (t == 0) {
+    hdr->sum_rule = red[0];
+    hdr->has_src = 1;
+  }
 }
 
 // Exclusive scan of the keep flags in three deterministic passes:

@@ -20,6 +20,7 @@
 #include "eval_f64.cuh"
 #include "eval_mixed.cuh"
 #include "build.cuh"
+#include "adjoint.cuh"
 #include "../../include/fastesp_b200.h"
 
 static_assert(FE_NCLASS <= FE_NCLASS_MAX, "class count");
@@ -122,7 +123,7 @@ EvalGeom eval_geom(int npts, int mode) {
 }
 
 struct Layout {
-  size_t off64[FE_NCLASS], off32[FE_NCLASS], off_atoms, bytes;
+  size_t off64[FE_NCLASS], off32[FE_NCLASS], off_atoms, off_src, bytes;
 };
 
 Layout table_layout(const int* cap, int n_atoms) {
@@ -137,7 +138,11 @@ Layout table_layout(const int* cap, int n_atoms) {
     t = align256(t + size_t(cap[L]) * fe_class_rec32[L] * 4);
   }
   l.off_atoms = t;
-  l.bytes = align256(t + size_t(n_atoms) * 4 * sizeof(double));
+  t = align256(t + size_t(n_atoms) * 4 * sizeof(double));
+  l.off_src = t;
+  size_t nrec = 0;
+  for (int L = 0; L < FE_NCLASS; ++L) nrec += size_t(cap[L]);
+  l.bytes = align256(t + nrec * sizeof(int));
   return l;
 }
 
@@ -157,6 +162,8 @@ int write_header(unsigned char* d_table, const int* cap, int n_atoms, const doub
     hdr.off32[L] = static_cast<long long>(lay.off32[L]);
   }
   hdr.off_atoms = static_cast<long long>(lay.off_atoms);
+  hdr.off_src = static_cast<long long>(lay.off_src);
+  hdr.has_src = 0;
   hdr.bytes = static_cast<long long>(lay.bytes);
   std::vector<unsigned char> h(sizeof hdr + size_t(n_atoms) * 4 * sizeof(double));
   memcpy(h.data(), &hdr, sizeof hdr);
@@ -194,7 +201,7 @@ struct fe_plan {
   size_t plan_bytes = 0;
   size_t table_bytes = 0;
   size_t o_tab64[FE_NCLASS], o_tab32[FE_NCLASS], o_atoms = 0;
-  size_t ws_stage = 0, ws_keep = 0, ws_pos = 0, ws_srule = 0, ws_bsum = 0;
+  size_t ws_stage = 0, ws_keep = 0, ws_pos = 0, ws_srule = 0, ws_swork = 0, ws_bsum = 0;
   long long nscan_blocks = 0;
   size_t ws_bytes = 0;
 };
@@ -342,6 +349,7 @@ int fe_plan_create(const fe_basis* b, fe_plan** out) {
   p->ws_keep = wput(size_t(p->nslot + 1) * sizeof(int));
   p->ws_pos = wput(size_t(p->nslot + 1) * sizeof(int));
   p->ws_srule = wput(size_t(p->nslot + 1) * sizeof(double));
+  p->ws_swork = wput(size_t(p->nslot + 1) * sizeof(int));
   p->nscan_blocks = (p->nslot + FE_SCAN_BLOCK - 1) / FE_SCAN_BLOCK;
   p->ws_bsum = wput(size_t(p->nscan_blocks + 1) * sizeof(int));
   p->ws_bytes = std::max<size_t>(w, 256);
@@ -427,6 +435,7 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
   a.stage_off = reinterpret_cast<const long long*>(pb + p->o_so);
   a.keep = reinterpret_cast<int*>(wb + p->ws_keep);
   a.srule = reinterpret_cast<double*>(wb + p->ws_srule);
+  a.swork = reinterpret_cast<int*>(wb + p->ws_swork);
   if (p->nblocks > 0) {
     fe_build_kernel<<<p->nblocks, FE_BUILD_THREADS, 0, st>>>(a);
     FE_CUDA(cudaGetLastError());
@@ -441,7 +450,7 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
     FE_CUDA(cudaGetLastError());
     const int thr = 256;
     fe_scatter_kernel<<<unsigned((p->nslot + thr - 1) / thr), thr, 0, st>>>(
-        a.stage, a.stage_off, a.class_slot0, FE_NCLASS, a.keep, pos, p->nslot, tb);
+        a.stage, a.stage_off, a.class_slot0, FE_NCLASS, a.keep, pos, a.swork, p->nslot, tb);
     FE_CUDA(cudaGetLastError());
   }
   fe_finalize_kernel<<<1, 1024, 0, st>>>(a.class_slot0, FE_NCLASS, p->nslot, a.keep, pos, a.srule, tb);
@@ -764,3 +773,209 @@ extern "C" int fe_esp_fp64_noalloc(const void* d_table, const double* d_pts, int
   return eval_launch("fe_esp_fp64_noalloc", d_table, d_pts, n_pts, d_out, scratch, need, 0, 0,
                      0.0, nullptr, st);
 }
+
+// ---------------------------------------------------------------------------
+// Field and adjoint
+// ---------------------------------------------------------------------------
+#ifndef FE_NPFIELD
+#define FE_NPFIELD 1
+#endif
+#ifndef FE_MINBFIELD
+#define FE_MINBFIELD 2
+#endif
+namespace {
+
+constexpr int kNPField = FE_NPFIELD, kMinBField = FE_MINBFIELD;
+
+struct FieldGeom {
+  int nblk_x, ld, split[2];
+  size_t plane() const { return size_t(split[0] + split[1]) * ld; }
+  size_t bytes() const { return align256(4 * plane() * sizeof(double)); }
+};
+
+FieldGeom field_geom(int npts) {
+  FieldGeom g{};
+  const int ppb = kEvalThreads * kNPField;
+  g.nblk_x = (npts + ppb - 1) / ppb;
+  const int target = 8 * kMinBField * sm_count();
+  g.split[0] = std::max(1, std::min(256, (target + g.nblk_x - 1) / std::max(1, g.nblk_x)));
+  g.split[1] = std::max(1, std::min(8, sm_count() / std::max(1, g.nblk_x)));
+  g.ld = (npts + 31) & ~31;
+  return g;
+}
+
+int field_launch(const char* who, const unsigned char* tb, const double* d_pts, int n_pts,
+                 const double* d_w, double* d_v, double* d_g, void* d_ws, size_t ws_bytes,
+                 cudaStream_t st) {
+  const FieldGeom g = field_geom(n_pts);
+  if (!d_ws || ws_bytes < g.bytes())
+    return fail(FE_ERR_SIZE, "%s: workspace too small (need at least %zu bytes)", who, g.bytes());
+  const int smem = FE_NSTAGE * FE_STAGE_BYTES;
+  FeFieldArgs a{};
+  a.table = tb;
+  a.pts = d_pts;
+  a.npts = n_pts;
+  a.ld = g.ld;
+  a.plane = g.plane();
+  auto k0 = fe_field_f64_kernel<kNPField, kEvalThreads, kMinBField, 0, FE_LSPLIT>;
+  auto k1 = fe_field_f64_kernel<kNPField, kEvalThreads, 1, FE_LSPLIT + 1, FE_NCLASS - 1>;
+  a.nsplit = g.split[0];
+  a.partial = static_cast<double*>(d_ws);
+  FE_CUDA(cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k0<<<dim3(g.nblk_x, g.split[0]), kEvalThreads, smem, st>>>(a);
+  FE_CUDA(cudaGetLastError());
+  a.nsplit = g.split[1];
+  a.partial = static_cast<double*>(d_ws) + size_t(g.split[0]) * g.ld;
+  FE_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k1<<<dim3(g.nblk_x, g.split[1]), kEvalThreads, smem, st>>>(a);
+  FE_CUDA(cudaGetLastError());
+  fe_field_reduce_kernel<<<(n_pts + 255) / 256, 256, 0, st>>>(
+      tb, d_pts, n_pts, static_cast<const double*>(d_ws), g.plane(), g.split[0] + g.split[1],
+      g.ld, d_w, d_v, d_g);
+  FE_CUDA(cudaGetLastError());
+  return FE_OK;
+}
+
+struct AdjLayout {
+  size_t field, mom, dw, first, last, bytes;
+  long long mom_off[FE_NCLASS];
+  long long nsrc;
+  int dw_stride;
+};
+
+AdjLayout adj_layout(const fe_plan* p, int n_pts) {
+  AdjLayout l{};
+  size_t o = 0;
+  auto put = [&](size_t bytes) { const size_t at = o; o = align256(o + bytes); return at; };
+  l.field = put(n_pts > 0 ? field_geom(n_pts).bytes() : 0);
+  long long nm = 0;
+  l.nsrc = 0;
+  for (int L = 0; L < FE_NCLASS; ++L) {
+    l.mom_off[L] = nm;
+    nm += (long long)p->cap[L] * fe_class_nterm[L];
+    l.nsrc += p->cap[L];
+  }
+  l.mom = put(size_t(nm) * sizeof(double));
+  int lmax = 0;
+  for (const FeShell& s : p->shells) lmax = std::max(lmax, s.l);
+  const int nc = (lmax + 1) * (lmax + 2) / 2;
+  l.dw_stride = nc * nc;
+  l.dw = put(size_t(l.nsrc) * l.dw_stride * sizeof(double));
+  l.first = put(p->tasks.size() * sizeof(int));
+  l.last = put(p->tasks.size() * sizeof(int));
+  l.bytes = std::max<size_t>(o, 256);
+  return l;
+}
+
+template <int L, int C>
+int launch_moments(const FeAdjArgs& a, int cap, cudaStream_t st) {
+  if constexpr (C < fe_mom_nchunk[L]) {
+    if (cap > 0)
+      fe_adj_moments_kernel<L, C><<<(cap + FE_ADJ_THREADS - 1) / FE_ADJ_THREADS, FE_ADJ_THREADS, 0,
+                                    st>>>(a);
+    FE_CUDA(cudaGetLastError());
+    return launch_moments<L, C + 1>(a, cap, st);
+  } else {
+    return FE_OK;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t fe_field_ws_bytes(int n_pts) {
+  if (n_pts <= 0) return 256;
+  return field_geom(n_pts).bytes();
+}
+
+int fe_esp_field_fp64(const void* d_table, const double* d_pts, int n_pts, const double* d_w,
+                      double* d_v, double* d_dvdc, void* d_ws, size_t ws_bytes, cudaStream_t st) {
+  if (n_pts < 0) return fail(FE_ERR_ARG, "fe_esp_field_fp64: n_pts < 0");
+  if (n_pts == 0) return FE_OK;
+  if (!d_table || !d_pts || (!d_v && !d_dvdc)) return fail(FE_ERR_ARG, "fe_esp_field_fp64: null argument");
+  return field_launch("fe_esp_field_fp64", static_cast<const unsigned char*>(d_table), d_pts,
+                      n_pts, d_w, d_v, d_dvdc, d_ws, ws_bytes, st);
+}
+
+size_t fe_adjoint_ws_bytes(const fe_plan* p, int n_pts) {
+  if (!p || n_pts < 0) return 0;
+  return adj_layout(p, n_pts).bytes;
+}
+
+int fe_esp_adjoint(const fe_plan* p, const void* d_plan, const void* d_table,
+                   const double* d_pts, int n_pts, const double* d_dLdV, double* d_dLdC,
+                   double* d_dLdP, void* d_ws, size_t ws_bytes, cudaStream_t st) {
+  if (!p || !d_table || n_pts < 0 || (n_pts > 0 && (!d_pts || !d_dLdV)))
+    return fail(FE_ERR_ARG, "fe_esp_adjoint: bad argument");
+  if (d_dLdP && !d_plan) return fail(FE_ERR_ARG, "fe_esp_adjoint: dL/dP needs the device plan");
+  const AdjLayout lay = adj_layout(p, n_pts);
+  if (!d_ws || ws_bytes < lay.bytes)
+    return fail(FE_ERR_SIZE, "fe_esp_adjoint: workspace %zu < %zu bytes", ws_bytes, lay.bytes);
+  if (reinterpret_cast<uintptr_t>(d_ws) & 255)
+    return fail(FE_ERR_ARG, "fe_esp_adjoint: workspace not 256-byte aligned");
+  const unsigned char* tb = static_cast<const unsigned char*>(d_table);
+  unsigned char* wb = static_cast<unsigned char*>(d_ws);
+  if (d_dLdP) {
+    // the table must come from a build with this plan (same capacities, sources filled)
+    FeTableHdr h{};
+    FE_CUDA(cudaMemcpyAsync(&h, tb, sizeof h, cudaMemcpyDeviceToHost, st));
+    FE_CUDA(cudaStreamSynchronize(st));
+    if (h.magic != FE_TABLE_MAGIC) return fail(FE_ERR_ARG, "fe_esp_adjoint: not a pair table");
+    if (!h.has_src)
+      return fail(FE_ERR_ARG, "fe_esp_adjoint: dL/dP needs a table built on the device "
+                  "(imported tables carry no pair sources)");
+    for (int L = 0; L < FE_NCLASS; ++L)
+      if (h.cap[L] != p->cap[L])
+        return fail(FE_ERR_ARG, "fe_esp_adjoint: table was not built with this plan");
+    FE_CUDA(cudaMemsetAsync(d_dLdP, 0, size_t(p->n_func) * p->n_func * sizeof(double), st));
+  }
+  if (n_pts == 0) return FE_OK;
+  if (d_dLdC) {
+    const int rc = field_launch("fe_esp_adjoint", tb, d_pts, n_pts, d_dLdV, nullptr, d_dLdC,
+                                wb + lay.field, lay.mom - lay.field, st);
+    if (rc != FE_OK) return rc;
+  }
+  if (!d_dLdP || lay.nsrc == 0) return FE_OK;
+  const unsigned char* pb = static_cast<const unsigned char*>(d_plan);
+  FeAdjArgs a{};
+  a.table = tb;
+  a.pts = d_pts;
+  a.w = d_dLdV;
+  a.npts = n_pts;
+  a.mom = reinterpret_cast<double*>(wb + lay.mom);
+  for (int L = 0; L < FE_NCLASS; ++L) a.mom_off[L] = lay.mom_off[L];
+  a.shells = reinterpret_cast<const FeShell*>(pb + p->o_shells);
+  a.sexp = reinterpret_cast<const double*>(pb + p->o_sexp);
+  a.scoef = reinterpret_cast<const double*>(pb + p->o_scoef);
+  a.tasks = reinterpret_cast<const FeTask*>(pb + p->o_tasks);
+  a.work_task = reinterpret_cast<const int*>(pb + p->o_wt);
+  a.work_ij = reinterpret_cast<const int*>(pb + p->o_wij);
+  a.n_func = p->n_func;
+  a.dw = reinterpret_cast<double*>(wb + lay.dw);
+  a.dw_stride = lay.dw_stride;
+  a.first = reinterpret_cast<int*>(wb + lay.first);
+  a.last = reinterpret_cast<int*>(wb + lay.last);
+  a.nsrc = lay.nsrc;
+  a.dD = d_dLdP;
+  int rc = FE_OK;
+#define FE_MOM(l) if (rc == FE_OK) rc = launch_moments<l, 0>(a, p->cap[l], st);
+  FE_MOM(0) FE_MOM(1) FE_MOM(2) FE_MOM(3) FE_MOM(4) FE_MOM(5) FE_MOM(6) FE_MOM(7) FE_MOM(8)
+#undef FE_MOM
+  if (rc != FE_OK) return rc;
+  const unsigned nb = unsigned((lay.nsrc + FE_ADJ_THREADS - 1) / FE_ADJ_THREADS);
+  fe_adj_pair_kernel<<<nb, FE_ADJ_THREADS, 0, st>>>(a);
+  FE_CUDA(cudaGetLastError());
+  const int ntask = int(p->tasks.size());
+  FE_CUDA(cudaMemsetAsync(a.first, 0xff, size_t(ntask) * sizeof(int), st));
+  fe_adj_ranges_kernel<<<nb, FE_ADJ_THREADS, 0, st>>>(a);
+  FE_CUDA(cudaGetLastError());
+  const long long nq = (long long)ntask * lay.dw_stride;
+  if (nq > 0) {
+    fe_adj_gather_kernel<<<unsigned((nq + 255) / 256), 256, 0, st>>>(a, ntask);
+    FE_CUDA(cudaGetLastError());
+  }
+  return FE_OK;
+}
+
+}  // extern "C"

@@ -9,7 +9,11 @@ For every angular class L = la + lb (0..8) this emits
   nested Horner form -- per Boys order m the polynomial sum_k G_k R^alpha_k is
   evaluated x-outer / y / z-inner with fused multiply-adds, every coefficient
   is read once and reused for the NP points;
-* ``fe_grad_L<L>``: the same sum and its gradient with respect to R (adjoint);
+* ``fe_grad_L<L>``: the same sum and its gradient with respect to R (field);
+* ``fe_mom_L<L>_c<c>``: the adjoint moments acc_k += w F_m_k R^alpha_k of one
+  chunk of the class's terms (terms in reference order, split at monomial
+  boundaries into chunks of at most MOM_CHUNK terms so the accumulators of a
+  chunk stay in registers);
 * the sparse contraction rows M0[k, t] (etab -> G) used by the table builder,
   with t in the compact order of ``hermite.t_index``;
 * the Boys Taylor grid F_n(i h), n = 0..NTAB-1, computed here in 40-digit
@@ -38,6 +42,7 @@ GRID_TMAX32 = 32.0             # FP32 grid covers 0 <= T < 32 (the FP32 asymptot
                                # thresholds of orders <= 6 lie below it)
 NTAB32 = MMAX + TAYLOR_K32
 VARS = ("x", "y", "z")
+MOM_CHUNK = 48                 # adjoint moment accumulators per thread
 
 
 # --------------------------------------------------------------------------
@@ -256,6 +261,67 @@ def grad_function(L):
     return out
 
 
+def mom_chunks(L):
+    """Contiguous term ranges [k0, k1) of class L (reference order), cut only
+    between monomials, as even as possible with at most MOM_CHUNK terms."""
+    keys, _ = H.class_terms(L)
+    bounds = [0]
+    for k in range(1, len(keys)):
+        if keys[k][:3] != keys[k - 1][:3]:
+            bounds.append(k)
+    nt = len(keys)
+    n = -(-nt // MOM_CHUNK)
+    while True:
+        cuts, last = [0], 0
+        for c in range(1, n):
+            want = nt * c / n
+            b = min((x for x in bounds if x > last), key=lambda x: abs(x - want), default=nt)
+            cuts.append(b)
+            last = b
+        cuts.append(nt)
+        spans = list(zip(cuts[:-1], cuts[1:]))
+        if all(0 < b - a <= MOM_CHUNK for a, b in spans):
+            return spans
+        n += 1
+
+
+def mom_function(L, c, k0, k1):
+    """acc[j] += R^alpha F_m w for the terms k0 + j of class L (wF[m] = w F_m)."""
+    keys, _ = H.class_terms(L)
+    sub = keys[k0:k1]
+    lines = [f"// class L={L} chunk {c}: terms [{k0}, {k1}) in reference order",
+             "template <typename Real>",
+             f"__device__ __forceinline__ void fe_mom_L{L}_c{c}(Real x, Real y, Real z,",
+             f"    const Real (&wF)[{L + 1}], Real (&acc)[{k1 - k0}]) {{"]
+    for ax, v in enumerate(VARS):
+        top = max(k[ax] for k in sub)
+        if top >= 1:
+            lines.append(f"  const Real {v}1 = {v};")
+        for e in range(2, top + 1):
+            lines.append(f"  const Real {v}{e} = {v}{e - 1} * {v};")
+    have_xy = set()
+    prev = None
+    fac, name = [], ""
+    for j, (a, b, cz, m) in enumerate(sub):
+        if (a, b, cz) != prev:
+            if a and b and (a, b) not in have_xy:
+                lines.append(f"  const Real x{a}y{b} = x{a} * y{b};")
+                have_xy.add((a, b))
+            fac = ([f"x{a}y{b}"] if a and b else ([f"x{a}"] if a else []) + ([f"y{b}"] if b else []))
+            fac += [f"z{cz}"] if cz else []
+            name = f"m{a}_{b}_{cz}"
+            if fac:
+                lines.append(f"  const Real {name} = {' * '.join(fac)};")
+            prev = (a, b, cz)
+        if fac:
+            lines.append(f"  acc[{j}] = fe_fma({name}, wF[{m}], acc[{j}]);")
+        else:
+            lines.append(f"  acc[{j}] += wF[{m}];")
+    lines.append("}")
+    lines.append("")
+    return lines
+
+
 # --------------------------------------------------------------------------
 # Boys grid and thresholds (40-digit reference values)
 # --------------------------------------------------------------------------
@@ -428,6 +494,32 @@ def main() -> int:
     for L in range(LMAX + 1):
         kw = "if" if L == 0 else "else if"
         out.append(f"  {kw} constexpr (L == {L}) fe_grad_L{L}<Real, NP>(g, x, y, z, F, s, u, dx, dy, dz);")
+    out.append("}")
+    out.append("")
+    # adjoint moment chunks
+    chunks = [mom_chunks(L) for L in range(LMAX + 1)]
+    nck = max(len(c) for c in chunks)
+    out.append(f"#define FE_MOM_MAXCHUNK {nck}")
+    out.append("static constexpr int fe_mom_nchunk[FE_NCLASS] = {"
+               + ", ".join(str(len(c)) for c in chunks) + "};")
+    for nm, idx in (("k0", 0), ("k1", 1)):
+        rows = ["{" + ", ".join(str(c[i][idx]) if i < len(c) else "0" for i in range(nck)) + "}"
+                for c in chunks]
+        out.append(f"static constexpr int fe_mom_{nm}[FE_NCLASS][FE_MOM_MAXCHUNK] = {{"
+                   + ", ".join(rows) + "};")
+    out.append("")
+    for L in range(LMAX + 1):
+        for c, (k0, k1) in enumerate(chunks[L]):
+            out += mom_function(L, c, k0, k1)
+    out.append("template <int L, int C, typename Real>")
+    out.append("__device__ __forceinline__ void fe_mom(Real x, Real y, Real z, const Real (&wF)[L + 1],")
+    out.append("    Real (&acc)[fe_mom_k1[L][C] - fe_mom_k0[L][C]]) {")
+    first = True
+    for L in range(LMAX + 1):
+        for c in range(len(chunks[L])):
+            kw = "if" if first else "else if"
+            first = False
+            out.append(f"  {kw} constexpr (L == {L} && C == {c}) fe_mom_L{L}_c{c}<Real>(x, y, z, wF, acc);")
     out.append("}")
     out.append("")
     out.append("__constant__ int fe_c_rec64[FE_NCLASS] = {"

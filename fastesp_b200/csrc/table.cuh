@@ -4,6 +4,7 @@
 //
 //   [FeTableHdr][pad to 256][class 0 FP64 records][class 1 ...]...[class 8]
 //                           [class 0 FP32 records]...[atoms: Z[n], xyz[3n]]
+//                           [sources: int32 per record slot, class 0 first]
 //
 // Pairs are grouped by angular class L = la + lb.  A class-L FP64 record is
 // fe_class_rec64[L] doubles: [p, Px, Py, Pz, K, K*bound, G_0 .. G_(nt-1), pad]
@@ -18,6 +19,11 @@
 // v as hi = float(v), lo = float(v - hi):
 // [p_hi, p_lo, Px_hi, Py_hi, Pz_hi, Px_lo, Py_lo, Pz_lo, K_hi, K_lo, K*bound,
 //  p^-1/2, G_hi[0..nt), G_lo[0..nt), pad to 16 bytes].
+//
+// The source section maps every record of a table built on the device back to
+// the builder's work item (shell pair and primitive indices), so the adjoint
+// can recompute the pair's Hermite coefficients; record i of class L has its
+// entry at sum_{L' < L} cap[L'] + i.  Imported tables have none (has_src 0).
 #pragma once
 #include <cstdint>
 
@@ -38,7 +44,8 @@ struct FeTableHdr {
   int64_t bytes;                     // total bytes of the table buffer
   double sum_rule;                   // Tr(P S) accumulated by the build
   int32_t has32;                     // FP32 records are current
-  int32_t pad_[3];
+  int32_t has_src;                   // the source section is filled
+  int64_t off_src;                   // byte offset of the source section
 };
 
 static_assert(sizeof(FeTableHdr) <= 512, "header must fit its slot");

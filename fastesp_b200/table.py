@@ -284,6 +284,69 @@ class PairTable:
         v = self._eval(points, "mixed", 0, tau=tau, n64=n64)
         return v, int(n64.item())
 
+    # -- derivatives ---------------------------------------------------
+    def esp_gradient(self, points=None, weights=None):
+        """(V, dV/dC) in FP64: the potential and its gradient with respect to
+        the points, (n,) and (n, 3); dV/dC is minus the electric field.  With
+        ``weights`` w (n,), the gradient rows are scaled by w (dL/dC for
+        dL/dV = w)."""
+        torch = _torch()
+        d, as_numpy = self._points(points)
+        n = int(d.shape[0])
+        v = torch.empty(n, dtype=torch.float64, device=self.device)
+        g = torch.empty((n, 3), dtype=torch.float64, device=self.device)
+        w = None if weights is None else _to_dev(weights, self.device).reshape(-1)
+        if w is not None and w.numel() != n:
+            raise ValueError(f"weights must have {n} entries, got {w.numel()}")
+        L = _lib.lib()
+        ws = _empty_bytes(int(L.fe_field_ws_bytes(n)), self.device)
+        _lib.check(L.fe_esp_field_fp64(_lib.ptr(self._buf), _lib.ptr(d), n, _lib.ptr(w),
+                                       _lib.ptr(v), _lib.ptr(g), _lib.ptr(ws), ws.numel(),
+                                       _lib.stream_ptr()))
+        if as_numpy:
+            return v.cpu().numpy(), g.cpu().numpy()
+        return v, g
+
+    def field(self, points=None):
+        """Electric field -dV/dC (n, 3), Hartree/(e Bohr)."""
+        v, g = self.esp_gradient(points)
+        return -g
+
+    def adjoint(self, points, dLdV, density: bool = True, coords: bool = True):
+        """Gradients of a loss L(V) with V = esp(points) and dL/dV given:
+        (dL/dP (n_func, n_func) or None, dL/dC (n, 3) or None), FP64, for the
+        Cartesian density P this table was built from; the kept pair set is held
+        fixed.  dL/dP needs a table built by build_table."""
+        torch = _torch()
+        if density and self.plan is None:
+            raise ValueError("dL/dP needs a table built by build_table (imported tables "
+                             "carry no pair sources)")
+        d, as_numpy = self._points(points)
+        n = int(d.shape[0])
+        w = _to_dev(dLdV, self.device).reshape(-1)
+        if w.numel() != n:
+            raise ValueError(f"dL/dV must have {n} entries, got {w.numel()}")
+        plan = self.plan
+        L = _lib.lib()
+        dP = (torch.empty((plan.n_func, plan.n_func), dtype=torch.float64, device=self.device)
+              if density else None)
+        dC = torch.empty((n, 3), dtype=torch.float64, device=self.device) if coords else None
+        if plan is not None:
+            nbytes = int(L.fe_adjoint_ws_bytes(plan._h, n))
+            ws = _empty_bytes(nbytes, self.device)
+            _lib.check(L.fe_esp_adjoint(plan._h, _lib.ptr(plan.d_plan), _lib.ptr(self._buf),
+                                        _lib.ptr(d), n, _lib.ptr(w), _lib.ptr(dC), _lib.ptr(dP),
+                                        _lib.ptr(ws), ws.numel(), _lib.stream_ptr()))
+        elif coords:
+            ws = _empty_bytes(int(L.fe_field_ws_bytes(n)), self.device)
+            _lib.check(L.fe_esp_field_fp64(_lib.ptr(self._buf), _lib.ptr(d), n, _lib.ptr(w),
+                                           None, _lib.ptr(dC), _lib.ptr(ws), ws.numel(),
+                                           _lib.stream_ptr()))
+        if as_numpy:
+            return (None if dP is None else dP.cpu().numpy(),
+                    None if dC is None else dC.cpu().numpy())
+        return dP, dC
+
     # -- export / import (pairs.bin) -----------------------------------
     def coefficients(self, L: int) -> np.ndarray:
         """(count, nt) G coefficients of class L in the reference's term order."""

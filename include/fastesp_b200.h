@@ -186,6 +186,34 @@ int fe_esp_fp64_noalloc(const void* d_table, const double* d_pts, int n_pts, dou
                         cudaStream_t stream);
 size_t fe_noalloc_scratch_bytes(void);
 
+/* Potential and its gradient with respect to the points, FP64 (no counterpart
+ * in the reference, which evaluates the potential only).  With R = C - P,
+ * dV/dC = sum_A -Z_A (C-R_A)/|C-R_A|^3
+ *         - sum_pairs K sum_k G_k (a R^(a-e) F_m - 2p R R^a F_(m+1))(pR^2),
+ * i.e. minus the electric field.  d_v (n, nullable) receives V; d_dvdc (n, 3,
+ * nullable) receives w_i dV_i/dC_i with w = d_w (n, nullable: w_i = 1).
+ * Workspace: fe_field_ws_bytes(n_pts). */
+size_t fe_field_ws_bytes(int n_pts);
+int fe_esp_field_fp64(const void* d_table, const double* d_pts, int n_pts, const double* d_w,
+                      double* d_v, double* d_dvdc, void* d_ws, size_t ws_bytes,
+                      cudaStream_t stream);
+
+/* Adjoint of V = table.esp(points) for a loss with dL/dV = d_dLdV (n), FP64
+ * (no counterpart in the reference).  d_dLdC (n, 3, nullable) receives
+ * dL/dC = dL/dV dV/dC; d_dLdP (n_func, n_func, nullable) receives dL/dP with
+ * respect to the Cartesian density given to fe_table_build: the per-pair
+ * point-weighted moments sum_i w_i R^a F_m are carried back through
+ * G = (2pi/p)(2p)^m M0 etab and etab = sum W c_a c_b Ex Ey Ez (the builder's
+ * contraction, fastesp/esp.py:239-250) to the density entries, with the kept
+ * pair set held fixed.  dL/dP needs a table built by fe_table_build with this
+ * plan; it reads the table header (one synchronising copy).  Deterministic:
+ * fixed summation orders, no atomics.  Workspace: fe_adjoint_ws_bytes(plan,
+ * n_pts), 256-byte aligned. */
+size_t fe_adjoint_ws_bytes(const fe_plan* plan, int n_pts);
+int fe_esp_adjoint(const fe_plan* plan, const void* d_plan, const void* d_table,
+                   const double* d_pts, int n_pts, const double* d_dLdV, double* d_dLdC,
+                   double* d_dLdP, void* d_ws, size_t ws_bytes, cudaStream_t stream);
+
 /* FMA throughput probe (no counterpart in the reference): ``blocks`` blocks of
  * 256 threads each run ``iters`` iterations of 8 independent FMA chains in FP64
  * (fp64 != 0) or FP32, writing one value per block to d_out.  Timed by the

@@ -328,6 +328,64 @@ class OracleTable:
                 out += (self.pp_K[sel[cs]][:, None] * acc).sum(0)
         return out
 
+    def electron_gradient(self, points=None) -> np.ndarray:
+        """d/dC of electron(C), (N, 3): the derivative of the sum in electron()
+        term by term, d/dC_c [R^a F_m(pR^2)] = a_c R^(a-e_c) F_m - 2p R_c R^a F_(m+1)
+        (R = C - P, dF_m/dT = -F_(m+1)); R^(a-e_c) is in the class's monomial
+        closure."""
+        pts = self.pts if points is None else np.asarray(points, float)
+        out = np.zeros((len(pts), 3))
+        nt = self.pp_nt
+        for n in np.unique(nt):
+            sel = np.nonzero(nt == n)[0]
+            off0 = self.pp_off[sel]
+            mo0 = self.pp_monooff[sel]
+            nm = int(self.pp_nmono[sel[0]])
+            par = self.mo_parent[mo0[0]:mo0[0] + nm]
+            axs = self.mo_axis[mo0[0]:mo0[0] + nm]
+            aidx = self.tm_aidx[off0[0]:off0[0] + n]
+            mm = self.tm_m[off0[0]:off0[0] + n]
+            exps = [(0, 0, 0)]
+            for j in range(1, nm):
+                e = list(exps[par[j]])
+                e[axs[j]] += 1
+                exps.append(tuple(e))
+            where = {e: j for j, e in enumerate(exps)}
+            g = self.tm_g[off0[:, None] + np.arange(n)[None, :]]
+            for c0 in range(0, len(sel), 2048):
+                cs = slice(c0, c0 + 2048)
+                P = np.stack([self.pp_cx[sel[cs]], self.pp_cy[sel[cs]], self.pp_cz[sel[cs]]], 1)
+                R = pts[None, :, :] - P[:, None, :]
+                pe = self.pp_exp[sel[cs]][:, None]
+                T = pe * np.einsum("cij,cij->ci", R, R)
+                F = [boys(k, T) for k in range(int(mm.max()) + 2)]
+                mono = [np.ones_like(T)]
+                for j in range(1, nm):
+                    mono.append(mono[par[j]] * R[:, :, axs[j]])
+                K = self.pp_K[sel[cs]][:, None]
+                for c in range(3):
+                    acc = np.zeros_like(T)
+                    for k in range(n):
+                        e = exps[aidx[k]]
+                        term = -2.0 * pe * R[:, :, c] * mono[aidx[k]] * F[mm[k] + 1]
+                        if e[c] > 0:
+                            d = list(e)
+                            d[c] -= 1
+                            term = term + e[c] * mono[where[tuple(d)]] * F[mm[k]]
+                        acc += g[cs, k][:, None] * term
+                    out[:, c] += (K * acc).sum(0)
+        return out
+
+    def esp_gradient(self, points=None) -> np.ndarray:
+        """dV/dC (N, 3) = d nuclear/dC - d electron/dC; minus the electric field."""
+        pts = self.pts if points is None else np.asarray(points, float)
+        g = -self.electron_gradient(pts)
+        for z, c in zip(self.Z, self.xyz):
+            d = pts - c
+            r = np.linalg.norm(d, axis=1)
+            g -= (z / r ** 3)[:, None] * d
+        return g
+
     def nuclear(self, points=None) -> np.ndarray:
         """sum_A Z_A/|C-R_A| (fastesp/table.py:95-100)."""
         pts = self.pts if points is None else np.asarray(points, float)

@@ -40,3 +40,11 @@ def small_system():
 @pytest.fixture(scope="session")
 def tz6_system():
     return load_golden_system("tz6")
+
+
+@pytest.fixture(scope="session")
+def frag54():
+    """The 54-atom l<=3 synthetic system (molecule seed 0): wfn, basis, density."""
+    from fastesp_b200 import synth
+    wfn, basis, P, _ = synth.load_workload("frag54", 10, seed=0)
+    return wfn, basis, P

@@ -112,12 +112,6 @@ def test_native_rule_matches_reference_builder(tag, request):
     assert tab.sum_rule == pytest.approx(float(g["native_sumrule"]), rel=1e-9)
 
 
-@pytest.fixture(scope="module")
-def frag54():
-    wfn, basis, P, _ = synth.load_workload("frag54", 10, seed=0)
-    return wfn, basis, P
-
-
 @pytest.mark.parametrize("tol,key", [(1e-12, "t12"), (0.0, "t0")])
 def test_frag54_300_matches_reference(frag54, golden, tol, key):
     """54-atom l<=3 system at the reference's own 300 points: parity bar 1e-10 a.u."""

@@ -103,3 +103,21 @@ def test_oracle_pairs_bin_roundtrip(tmp_path, small_system):
     back = O.OracleTable.read(tmp_path / "pairs.bin")
     for k in ("pp_exp", "pp_K", "tm_g", "tm_aidx", "mo_parent", "pts", "Z", "xyz"):
         np.testing.assert_array_equal(getattr(back, k), getattr(tab, k))
+
+
+def test_oracle_gradient_matches_central_differences(small_system):
+    """The oracle's term-by-term field formula against central differences of
+    its own potential (the pin for the GPU field and adjoint tests)."""
+    wfn, basis, P, g = small_system
+    Z = np.array([Z_OF[s] for s in wfn.symbols])
+    pts = g["points"][:12]
+    tab = O.build_table(wfn.shells, wfn.coords, Z, g["density"], pts, tol=1e-12)
+    an = tab.esp_gradient(pts)
+    h = 1e-5
+    fd = np.zeros_like(an)
+    for c in range(3):
+        d = np.zeros_like(pts)
+        d[:, c] = h
+        fd[:, c] = (tab.esp(pts + d) - tab.esp(pts - d)) / (2 * h)
+    scale = np.maximum(np.abs(an), 1e-3 * np.abs(an).max())
+    assert (np.abs(fd - an) / scale).max() < 1e-6
