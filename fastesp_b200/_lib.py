@@ -47,6 +47,15 @@ class FeTableInfo(C.Structure):
                 ("has_f32", C.c_int)]
 
 
+class FeBatchMol(C.Structure):
+    _fields_ = [("d_table", C.c_void_p), ("d_pts", C.c_void_p), ("d_out", C.c_void_p),
+                ("n_pts", C.c_int), ("reserved", C.c_int)]
+
+
+class FeBatchShape(C.Structure):
+    _fields_ = [("points_per_thread", C.c_int), ("waves", C.c_int)]
+
+
 _P = C.c_void_p
 _SIGS = {
     "fe_version": (C.c_int, []),
@@ -79,6 +88,13 @@ _SIGS = {
     "fe_esp_field_fp64": (C.c_int, [_P, _P, C.c_int, _P, _P, _P, _P, C.c_size_t, _P]),
     "fe_adjoint_ws_bytes": (C.c_size_t, [_P, C.c_int]),
     "fe_esp_adjoint": (C.c_int, [_P, _P, _P, _P, C.c_int, _P, _P, _P, _P, C.c_size_t, _P]),
+    "fe_batch_create": (C.c_int, [C.POINTER(FeBatchMol), C.c_int, C.POINTER(FeBatchShape),
+                                  C.POINTER(_P), _P]),
+    "fe_batch_destroy": (None, [_P]),
+    "fe_batch_sizes": (C.c_int, [_P, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
+                                 C.POINTER(C.c_int)]),
+    "fe_batch_upload": (C.c_int, [_P, _P, C.c_size_t, _P]),
+    "fe_batch_run": (C.c_int, [_P, _P, _P, C.c_size_t, _P]),
 }
 
 _lock = threading.Lock()

@@ -92,6 +92,10 @@ FE_DEV void fe_item(const FeBlockWork& w, const int* tile_sz, int i, int& L, int
 // mbarriers; every thread waits for the current stage, evaluates it, and the
 // block releases it (a barrier) before thread 0 refills it.  ``elem`` bytes per
 // record word, class record words ``rec[L]``, class byte offsets ``off[L]``.
+// A persistent block runs several work items through one ring: ``base`` counts
+// the tiles of its earlier items, so stage and phase continue from them and the
+// mbarriers are initialised once (every issued tile is waited on before an
+// item ends, so the ring is idle between items).
 struct FeTilePipe {
   const unsigned char* table;
   const int* tile_sz;
@@ -106,21 +110,29 @@ struct FeTilePipe {
   const int* rec2 = nullptr;
   const int64_t* off2 = nullptr;
   int elem2 = 0;
+  int base = 0;
 
-  FE_DEV void start(const FeTableHdr* hdr, int split, int nsplit, int llo, int lhi, int align = 1) {
+  FE_DEV void init_barriers() const {
     if (threadIdx.x == 0) {
-      fe_block_work(hdr, split, nsplit, tile_sz, llo, lhi, *w, align);
       for (int s = 0; s < FE_NSTAGE; ++s) mbar_init(&bar[s], 1);
       mbar_fence_init();
     }
+  }
+  // Work split of this item (thread 0), then the first FE_NSTAGE copies.
+  FE_DEV void begin(const FeTableHdr* hdr, int split, int nsplit, int llo, int lhi, int align = 1) {
+    if (threadIdx.x == 0) fe_block_work(hdr, split, nsplit, tile_sz, llo, lhi, *w, align);
     __syncthreads();
     if (threadIdx.x == 0)
       for (int i = 0; i < FE_NSTAGE && i < w->total; ++i) issue(i);
   }
+  FE_DEV void start(const FeTableHdr* hdr, int split, int nsplit, int llo, int lhi, int align = 1) {
+    init_barriers();
+    begin(hdr, split, nsplit, llo, lhi, align);
+  }
   FE_DEV void issue(int i) const {
     int L, first, n;
     fe_item(*w, tile_sz, i, L, first, n);
-    const int s = i % FE_NSTAGE;
+    const int s = (base + i) % FE_NSTAGE;
     const unsigned bytes = unsigned(n) * unsigned(rec[L]) * unsigned(elem);
     const unsigned bytes2 = rec2 ? unsigned(n) * unsigned(rec2[L]) * unsigned(elem2) : 0u;
     mbar_expect_tx(&bar[s], bytes + bytes2);
@@ -132,10 +144,13 @@ struct FeTilePipe {
   }
   // Wait for tile i; false (for every thread) if the wait gave up.
   FE_DEV bool wait(int i) const {
-    const bool got = mbar_wait_bounded(&bar[i % FE_NSTAGE], (i / FE_NSTAGE) & 1);
+    const int g = base + i;
+    const bool got = mbar_wait_bounded(&bar[g % FE_NSTAGE], (g / FE_NSTAGE) & 1);
     return !__syncthreads_or(!got);
   }
-  FE_DEV const unsigned char* stage(int i) const { return smem + (i % FE_NSTAGE) * FE_STAGE_BYTES; }
+  FE_DEV const unsigned char* stage(int i) const {
+    return smem + ((base + i) % FE_NSTAGE) * FE_STAGE_BYTES;
+  }
   FE_DEV void release(int i) const {
     __syncthreads();
     if (threadIdx.x == 0 && i + FE_NSTAGE < w->total) issue(i + FE_NSTAGE);
@@ -143,8 +158,10 @@ struct FeTilePipe {
   // After a failed wait at tile i: drain the copies still in flight.
   FE_DEV void abort(int i) const {
     if (threadIdx.x == 0)
-      for (int k = i + 1; k < i + FE_NSTAGE && k < w->total; ++k)
-        mbar_wait_bounded(&bar[k % FE_NSTAGE], (k / FE_NSTAGE) & 1);
+      for (int k = i + 1; k < i + FE_NSTAGE && k < w->total; ++k) {
+        const int g = base + k;
+        mbar_wait_bounded(&bar[g % FE_NSTAGE], (g / FE_NSTAGE) & 1);
+      }
     __syncthreads();
   }
 };

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstddef>
 #include <cstdio>
@@ -21,6 +22,7 @@
 #include "eval_mixed.cuh"
 #include "build.cuh"
 #include "adjoint.cuh"
+#include "batch.cuh"
 #include "../../include/fastesp_b200.h"
 
 static_assert(FE_NCLASS <= FE_NCLASS_MAX, "class count");
@@ -975,6 +977,208 @@ int fe_esp_adjoint(const fe_plan* p, const void* d_plan, const void* d_table,
     fe_adj_gather_kernel<<<unsigned((nq + 255) / 256), 256, 0, st>>>(a, ntask);
     FE_CUDA(cudaGetLastError());
   }
+  return FE_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched evaluation
+// ---------------------------------------------------------------------------
+struct fe_batch {
+  int np = 2, n_inst = 1;
+  int grid[2] = {1, 1};
+  std::vector<FeBatchMolDev> mols;
+  std::vector<FeBatchItem> items;
+  long long total_pts = 0;
+  size_t partial_doubles = 0;
+  size_t desc_bytes = 0, ws_bytes = 0;
+  size_t off_mol = 0, off_item = 0;
+};
+
+namespace {
+
+constexpr size_t kBatchCounterBytes = 256;   // two counters, one per kernel instance
+
+template <int NP>
+struct BatchKernels {
+  static constexpr int kMinB = NP == 1 ? 4 : kMinB64;
+  static const void* main() {
+    return reinterpret_cast<const void*>(fe_batch_f64_kernel<NP, kMinB, 0, FE_LSPLIT, 0>);
+  }
+  static const void* high() {
+    return reinterpret_cast<const void*>(fe_batch_f64_kernel<NP, 1, FE_LSPLIT + 1, FE_NCLASS - 1, 1>);
+  }
+};
+
+int batch_kernels(int np, const void*& k0, const void*& k1) {
+  if (np == 1) { k0 = BatchKernels<1>::main(); k1 = BatchKernels<1>::high(); return FE_OK; }
+  if (np == 2) { k0 = BatchKernels<2>::main(); k1 = BatchKernels<2>::high(); return FE_OK; }
+  return fail(FE_ERR_ARG, "fe_batch_create: points_per_thread must be 1 or 2");
+}
+
+// Algorithmic FLOPs of one (pair, point) evaluation of class L.
+double pair_point_flops(int L) {
+  const int nmono = (L + 1) * (L + 2) * (L + 3) / 6;
+  return 2.0 * fe_class_nterm[L] + (nmono - 1) + 14 + 3 * L;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fe_batch_create(const fe_batch_mol* in, int n_mol, const fe_batch_shape* shape,
+                    fe_batch** out, cudaStream_t st) {
+  if (!out || n_mol < 0 || (n_mol > 0 && !in)) return fail(FE_ERR_ARG, "fe_batch_create: bad argument");
+  *out = nullptr;
+  const int np = shape ? shape->points_per_thread : 2;
+  const int waves = shape ? shape->waves : 4;
+  if (waves < 1 || waves > 64) return fail(FE_ERR_ARG, "fe_batch_create: waves must be in 1..64");
+  const void* k0 = nullptr;
+  const void* k1 = nullptr;
+  {
+    const int rc = batch_kernels(np, k0, k1);
+    if (rc != FE_OK) return rc;
+  }
+  const int smem = FE_NSTAGE * FE_STAGE_BYTES;
+  FE_CUDA(cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  FE_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int occ0 = 0, occ1 = 0;
+  FE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, k0, 128, smem));
+  FE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, k1, 128, smem));
+  occ0 = std::max(occ0, 1);
+  occ1 = std::max(occ1, 1);
+
+  auto* b = new fe_batch();
+  b->np = np;
+  const int ppb = 128 * np;
+  std::vector<double> work(n_mol, 0.0);   // FLOPs per point of each molecule
+  std::vector<int> npairs(n_mol, 0);
+  double total = 0.0;
+  for (int m = 0; m < n_mol; ++m) {
+    if (in[m].n_pts < 0 || (in[m].n_pts > 0 && (!in[m].d_table || !in[m].d_pts || !in[m].d_out))) {
+      delete b;
+      return fail(FE_ERR_ARG, "fe_batch_create: molecule %d: bad buffers", m);
+    }
+    if (!in[m].d_table) continue;
+    FeTableHdr h{};
+    FE_CUDA(cudaMemcpyAsync(&h, in[m].d_table, sizeof h, cudaMemcpyDeviceToHost, st));
+    FE_CUDA(cudaStreamSynchronize(st));
+    if (h.magic != FE_TABLE_MAGIC) {
+      delete b;
+      return fail(FE_ERR_ARG, "fe_batch_create: molecule %d: not a pair table", m);
+    }
+    for (int L = 0; L < FE_NCLASS; ++L) {
+      work[m] += h.count[L] * pair_point_flops(L);
+      npairs[m] += h.count[L];
+      if (L > FE_LSPLIT && h.count[L] > 0) b->n_inst = 2;
+    }
+    total += work[m] * in[m].n_pts;
+  }
+  // pair splits: items of about equal cost, ``waves`` items per resident block
+  const double target_items = double(waves) * occ0 * sm_count();
+  const double item_cost = std::max(1.0, total / target_items);
+  long long base = 0, pt0 = 0;
+  for (int m = 0; m < n_mol; ++m) {
+    FeBatchMolDev d{};
+    d.table = static_cast<const unsigned char*>(in[m].d_table);
+    d.pts = in[m].d_pts;
+    d.out = in[m].d_out;
+    d.npts = in[m].n_pts;
+    int ns = int(std::ceil(ppb * work[m] / item_cost));
+    ns = std::max(1, std::min({ns, 256, std::max(1, npairs[m] / 32)}));
+    d.nsplit = ns;
+    d.ld = (std::max(d.npts, 1) + 31) & ~31;
+    d.nrows = ns * b->n_inst;
+    d.base = base;
+    d.pt0 = pt0;
+    if (d.npts > 0) {
+      base += (long long)d.nrows * d.ld;
+      pt0 += d.npts;
+      const int nb = (d.npts + ppb - 1) / ppb;
+      for (int pb = 0; pb < nb; ++pb)
+        for (int s = 0; s < ns; ++s) b->items.push_back(FeBatchItem{m, pb, s, 0});
+    }
+    b->mols.push_back(d);
+  }
+  // largest first (stable, so the order is deterministic)
+  auto cost = [&](const FeBatchItem& it) {
+    const FeBatchMolDev& d = b->mols[it.mol];
+    const int pts = std::min(ppb, d.npts - it.pblock * ppb);
+    return double(pts) * work[it.mol] / d.nsplit;
+  };
+  std::stable_sort(b->items.begin(), b->items.end(),
+                   [&](const FeBatchItem& x, const FeBatchItem& y) { return cost(x) > cost(y); });
+  b->total_pts = pt0;
+  b->partial_doubles = size_t(base);
+  const int nit = int(b->items.size());
+  b->grid[0] = std::max(1, std::min(nit, occ0 * sm_count()));
+  b->grid[1] = std::max(1, std::min(nit, occ1 * sm_count()));
+  b->off_mol = align256(sizeof(FeBatchHdr));
+  b->off_item = align256(b->off_mol + b->mols.size() * sizeof(FeBatchMolDev));
+  b->desc_bytes = align256(b->off_item + b->items.size() * sizeof(FeBatchItem));
+  b->ws_bytes = kBatchCounterBytes + align256(b->partial_doubles * sizeof(double));
+  *out = b;
+  return FE_OK;
+}
+
+void fe_batch_destroy(fe_batch* b) { delete b; }
+
+int fe_batch_sizes(const fe_batch* b, size_t* desc_bytes, size_t* ws_bytes, int* n_items) {
+  if (!b) return fail(FE_ERR_ARG, "fe_batch_sizes: null batch");
+  if (desc_bytes) *desc_bytes = b->desc_bytes;
+  if (ws_bytes) *ws_bytes = b->ws_bytes;
+  if (n_items) *n_items = int(b->items.size());
+  return FE_OK;
+}
+
+int fe_batch_upload(const fe_batch* b, void* d_desc, size_t desc_bytes, cudaStream_t st) {
+  if (!b || !d_desc) return fail(FE_ERR_ARG, "fe_batch_upload: null argument");
+  if (desc_bytes < b->desc_bytes) return fail(FE_ERR_SIZE, "fe_batch_upload: %zu < %zu bytes", desc_bytes, b->desc_bytes);
+  if (reinterpret_cast<uintptr_t>(d_desc) & 255) return fail(FE_ERR_ARG, "fe_batch_upload: descriptor not 256-byte aligned");
+  std::vector<unsigned char> h(b->desc_bytes, 0);
+  FeBatchHdr hdr{};
+  hdr.n_mol = int(b->mols.size());
+  hdr.n_item = int(b->items.size());
+  hdr.np = b->np;
+  hdr.n_inst = b->n_inst;
+  hdr.total_pts = b->total_pts;
+  hdr.off_mol = static_cast<long long>(b->off_mol);
+  hdr.off_item = static_cast<long long>(b->off_item);
+  memcpy(h.data(), &hdr, sizeof hdr);
+  if (!b->mols.empty()) memcpy(h.data() + b->off_mol, b->mols.data(), b->mols.size() * sizeof(FeBatchMolDev));
+  if (!b->items.empty()) memcpy(h.data() + b->off_item, b->items.data(), b->items.size() * sizeof(FeBatchItem));
+  FE_CUDA(cudaMemcpyAsync(d_desc, h.data(), h.size(), cudaMemcpyHostToDevice, st));
+  FE_CUDA(cudaStreamSynchronize(st));   // h is a local buffer
+  return FE_OK;
+}
+
+int fe_batch_run(const fe_batch* b, const void* d_desc, void* d_ws, size_t ws_bytes, cudaStream_t st) {
+  if (!b || !d_desc) return fail(FE_ERR_ARG, "fe_batch_run: null argument");
+  if (b->items.empty()) return FE_OK;
+  if (!d_ws || ws_bytes < b->ws_bytes) return fail(FE_ERR_SIZE, "fe_batch_run: workspace too small (need %zu bytes)", b->ws_bytes);
+  const void* k0 = nullptr;
+  const void* k1 = nullptr;
+  {
+    const int rc = batch_kernels(b->np, k0, k1);
+    if (rc != FE_OK) return rc;
+  }
+  unsigned char* wb = static_cast<unsigned char*>(d_ws);
+  unsigned* counter = reinterpret_cast<unsigned*>(wb);
+  double* partial = reinterpret_cast<double*>(wb + kBatchCounterBytes);
+  const unsigned char* desc = static_cast<const unsigned char*>(d_desc);
+  FE_CUDA(cudaMemsetAsync(counter, 0, kBatchCounterBytes, st));
+  const int smem = FE_NSTAGE * FE_STAGE_BYTES;
+  unsigned* c1 = counter + 32;
+  void* a0[] = {&desc, &counter, &partial};
+  FE_CUDA(cudaLaunchKernel(k0, dim3(b->grid[0]), dim3(128), a0, smem, st));
+  if (b->n_inst == 2) {
+    void* a1[] = {&desc, &c1, &partial};
+    FE_CUDA(cudaLaunchKernel(k1, dim3(b->grid[1]), dim3(128), a1, smem, st));
+  }
+  if (b->total_pts > 0)
+    fe_batch_reduce_kernel<<<unsigned((b->total_pts + 255) / 256), 256, 0, st>>>(desc, partial);
+  FE_CUDA(cudaGetLastError());
   return FE_OK;
 }
 

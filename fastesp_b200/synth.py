@@ -272,6 +272,20 @@ def load_workload(name: str, n_points: int, seed: int = 0, points_seed: int = 1,
     return wfn, basis, dens, pts
 
 
+def batch_workload(n_mol: int = 64, seed: int = 0):
+    """The uneven batch: ``n_mol`` molecules with atom counts uniform in [5, 60],
+    l<=2 bases, and 200-5000 surface points each (log-uniform).  Returns a list
+    of (wfn, basis, density, points)."""
+    rng = np.random.default_rng([seed, 4242])
+    out = []
+    for i in range(n_mol):
+        natom = int(rng.integers(5, 61))
+        npts = int(round(np.exp(rng.uniform(np.log(200.0), np.log(5000.0)))))
+        out.append(load_workload("batch", npts, seed=1000 * seed + i, points_seed=i + 1,
+                                 natom=natom))
+    return out
+
+
 def digest(*arrays) -> str:
     h = hashlib.sha256()
     for a in arrays:

@@ -214,6 +214,40 @@ int fe_esp_adjoint(const fe_plan* plan, const void* d_plan, const void* d_table,
                    const double* d_pts, int n_pts, const double* d_dLdV, double* d_dLdC,
                    double* d_dLdP, void* d_ws, size_t ws_bytes, cudaStream_t stream);
 
+/* Batched FP64 evaluation (no counterpart in the reference, which runs one
+ * molecule per process): V for many molecules, each with its own table and
+ * points, in one persistent launch over a flattened queue of
+ * (molecule, point block, pair split) work items ordered largest first and
+ * claimed by the resident blocks from a global counter.  Same per-point
+ * arithmetic as fe_esp_fp64; deterministic.  Use: fe_batch_create (reads
+ * every table's header: synchronising), fe_batch_sizes, a caller-allocated
+ * descriptor filled by fe_batch_upload, then fe_batch_run any number of times
+ * (stream-ordered, no synchronisation or allocation: it can be captured in a
+ * CUDA graph) with a workspace of the reported size.  The buffers named in
+ * ``mols`` must stay valid while the batch is used. */
+typedef struct fe_batch_mol {
+  const void* d_table;          /* pair table (fe_table_build / fe_table_init) */
+  const double* d_pts;          /* (n_pts, 3) Bohr */
+  double* d_out;                /* (n_pts) V */
+  int n_pts;
+  int reserved;
+} fe_batch_mol;
+
+typedef struct fe_batch_shape {
+  int points_per_thread;        /* 1 or 2: point block of 128 or 256 points */
+  int waves;                    /* work items per resident block, 1..64 */
+} fe_batch_shape;
+
+typedef struct fe_batch fe_batch;   /* opaque, host memory */
+
+int fe_batch_create(const fe_batch_mol* mols, int n_mol, const fe_batch_shape* shape,
+                    fe_batch** out, cudaStream_t stream);
+void fe_batch_destroy(fe_batch* batch);
+int fe_batch_sizes(const fe_batch* batch, size_t* desc_bytes, size_t* ws_bytes, int* n_items);
+int fe_batch_upload(const fe_batch* batch, void* d_desc, size_t desc_bytes, cudaStream_t stream);
+int fe_batch_run(const fe_batch* batch, const void* d_desc, void* d_ws, size_t ws_bytes,
+                 cudaStream_t stream);
+
 /* FMA throughput probe (no counterpart in the reference): ``blocks`` blocks of
  * 256 threads each run ``iters`` iterations of 8 independent FMA chains in FP64
  * (fp64 != 0) or FP32, writing one value per block to d_out.  Timed by the
