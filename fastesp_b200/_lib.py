@@ -67,6 +67,7 @@ _SIGS = {
     "fe_plan_upload": (C.c_int, [_P, _P, _P]),
     "fe_table_build": (C.c_int, [_P, _P, _P, _P, C.c_int, C.c_double, C.c_int, _P, _P,
                                  C.c_size_t, _P]),
+    "fe_build_ws_bytes": (C.c_size_t, [_P, C.c_int]),
     "fe_table_bytes": (C.c_size_t, [C.POINTER(C.c_int), C.c_int]),
     "fe_table_offsets": (C.c_int, [C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_size_t),
                                    C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),

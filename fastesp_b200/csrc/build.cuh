@@ -14,7 +14,9 @@
 //   G_k = (2 pi/p)(2p)^m_k sum_t M0[k,t] etab[t]              (esp.py:248-250),
 //         stored at record position fe_gpos_L[k] (the order the kernels read them)
 //   bound = (2p)^-1.5 sum_t |etab_t| M_tx M_ty M_tz (2p)^(|t|/2), reff = 1.6 sqrt((L+2)/p)
-//   screen: rule 0 keeps unless K bound / max(dmin, 0.05) < tol   (table.py:190-194)
+//   screen: rule 0 keeps unless K bound / max(dmin, 0.05) < tol   (table.py:190-194);
+//           dmin is the exact nearest-point distance, found by a pruned search
+//           over point-block bounding boxes
 //           rule 1 drops if K bound / max(dmin - reff, 0.05) < tol,
 //                  and drops pairs with c_a c_b == 0 or all G == 0 (build_pairs.cpp:243,309,326-328)
 #pragma once
@@ -49,6 +51,9 @@ struct FeBuildArgs {
   const double* dens;            // (n_func, n_func) Cartesian density
   const double* pts;             // (npts, 3)
   int npts;
+  const double* box;             // per 32-point block: lo xyz, hi xyz (6 doubles)
+  const double* sbox;            // per 32-block superblock: the same
+  int nbox, nsbox;
   double tol;
   int rule;
   const long long* class_slot0;  // first global slot of class L in the staging arrays
@@ -121,6 +126,58 @@ FE_DEV const signed char* fe_m0_m() {
   else if constexpr (L == 4) return fe_m0_m_L4; else if constexpr (L == 5) return fe_m0_m_L5;
   else if constexpr (L == 6) return fe_m0_m_L6; else if constexpr (L == 7) return fe_m0_m_L7;
   else return fe_m0_m_L8;
+}
+
+// Squared distance from P to the box [lo, hi] (0 inside); a lower bound of the
+// squared distance to every point in it.
+FE_DEV double fe_box_lb2(const double* __restrict__ b, const double (&P)[3]) {
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double g = fmax(fmax(b[k] - P[k], P[k] - b[3 + k]), 0.0);
+    s += g * g;
+  }
+  return s;
+}
+
+// Bounding boxes of consecutive 32-point blocks (level 0: points -> boxes) and
+// of 32-box superblocks (level 1: boxes -> superboxes).  One thread per box.
+__global__ void fe_point_boxes_kernel(const double* __restrict__ pts, int npts, double* box,
+                                      int nbox) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbox) return;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  const int q1 = min(32 * b + 32, npts);
+  for (int q = 32 * b; q < q1; ++q)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = fmin(lo[k], pts[3 * q + k]);
+      hi[k] = fmax(hi[k], pts[3 * q + k]);
+    }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    box[6 * b + k] = lo[k];
+    box[6 * b + 3 + k] = hi[k];
+  }
+}
+
+__global__ void fe_super_boxes_kernel(const double* __restrict__ box, int nbox, double* sbox,
+                                      int nsbox) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsbox) return;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  const int b1 = min(32 * s + 32, nbox);
+  for (int b = 32 * s; b < b1; ++b)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = fmin(lo[k], box[6 * b + k]);
+      hi[k] = fmax(hi[k], box[6 * b + 3 + k]);
+    }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    sbox[6 * s + k] = lo[k];
+    sbox[6 * s + 3 + k] = hi[k];
+  }
 }
 
 // E[i][j][t] of (u + xa)^i (u + xb)^j exp(-p u^2), i <= LA, j <= LB, t <= LA+LB.
@@ -274,26 +331,51 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
   const double bound = pow(tp, -1.5) * bsum;
   const double reff = 1.6 * sqrt((L + 2.0) / p);
 
-  // nearest point (exact IEEE arithmetic, no contraction, as NumPy does)
+  // Nearest point, exactly as the reference computes it (IEEE arithmetic, no
+  // contraction: the minimum of ((dx^2 + dy^2) + dz^2) over the points), found
+  // by a search over 1024-point superblocks and 32-point blocks that skips a
+  // box whose distance lower bound exceeds the best distance so far -- the
+  // minimum is the brute-force one -- and stops early once the pair is kept
+  // whatever the remaining points are (the bound test below, with a 1e-9
+  // relative margin far above rounding).
+  const double KB = __dmul_rn(K, bound);
   double d2min = 1e300;
-  for (int q = 0; q < a.npts; ++q) {
-    const double dx = __dsub_rn(a.pts[3 * q], P[0]);
-    const double dy = __dsub_rn(a.pts[3 * q + 1], P[1]);
-    const double dz = __dsub_rn(a.pts[3 * q + 2], P[2]);
-    const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-    d2min = fmin(d2min, d2);
+  bool sure = false;
+  auto sure_keep = [&](double d2) {
+    double d = __dsqrt_rn(d2);
+    if (a.rule == 1) d = d - reff;
+    return KB >= a.tol * (1.0 + 1e-9) * fmax(d, 0.05);
+  };
+  for (int sb = 0; sb < a.nsbox && !sure; ++sb) {
+    if (fe_box_lb2(a.sbox + 6 * sb, P) * (1.0 - 1e-12) > d2min) continue;
+    const int b1 = min(32 * sb + 32, a.nbox);
+    for (int b = 32 * sb; b < b1; ++b) {
+      if (fe_box_lb2(a.box + 6 * b, P) * (1.0 - 1e-12) > d2min) continue;
+      const int q1 = min(32 * b + 32, a.npts);
+      for (int q = 32 * b; q < q1; ++q) {
+        const double dx = __dsub_rn(a.pts[3 * q], P[0]);
+        const double dy = __dsub_rn(a.pts[3 * q + 1], P[1]);
+        const double dz = __dsub_rn(a.pts[3 * q + 2], P[2]);
+        const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+        d2min = fmin(d2min, d2);
+      }
+      if (sure_keep(d2min)) {
+        sure = true;
+        break;
+      }
+    }
   }
   double dd = __dsqrt_rn(d2min);
   if (a.rule == 1) dd = dd - reff;
   dd = fmax(dd, 0.05);
-  const bool keep = a.npts == 0 ? true : !(__ddiv_rn(__dmul_rn(K, bound), dd) < a.tol);
+  const bool keep = a.npts == 0 || sure ? true : !(__ddiv_rn(KB, dd) < a.tol);
   if (!keep) return;
   rec[0] = p;
   rec[1] = P[0];
   rec[2] = P[1];
   rec[3] = P[2];
   rec[4] = K;
-  rec[5] = __dmul_rn(K, bound);
+  rec[5] = KB;
 #pragma unroll
   for (int k = 6 + NT; k < REC; ++k) rec[k] = 0.0;
   a.keep[slot] = 1;

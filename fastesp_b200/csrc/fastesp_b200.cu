@@ -395,6 +395,12 @@ int fe_plan_upload(const fe_plan* p, void* d_plan, cudaStream_t st) {
   return FE_OK;
 }
 
+size_t fe_build_ws_bytes(const fe_plan* p, int n_pts) {
+  if (!p || n_pts < 0) return 0;
+  const size_t nbox = (size_t(n_pts) + 31) / 32, nsbox = (nbox + 31) / 32;
+  return p->ws_bytes + align256(nbox * 6 * sizeof(double)) + align256(nsbox * 6 * sizeof(double));
+}
+
 int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
                    const double* d_pts, int n_pts, double tol, int rule, void* d_table,
                    void* d_ws, size_t ws_bytes, cudaStream_t st) {
@@ -403,7 +409,8 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
   if (n_pts < 0 || (n_pts > 0 && !d_pts)) return fail(FE_ERR_ARG, "fe_table_build: bad points");
   if (rule != FE_RULE_NUMPY && rule != FE_RULE_NATIVE) return fail(FE_ERR_ARG, "fe_table_build: unknown rule %d", rule);
   if (!(tol >= 0.0)) return fail(FE_ERR_ARG, "fe_table_build: tol must be >= 0");
-  if (ws_bytes < p->ws_bytes) return fail(FE_ERR_SIZE, "fe_table_build: workspace %zu < %zu bytes", ws_bytes, p->ws_bytes);
+  const size_t need = fe_build_ws_bytes(p, n_pts);
+  if (ws_bytes < need) return fail(FE_ERR_SIZE, "fe_table_build: workspace %zu < %zu bytes (fe_build_ws_bytes)", ws_bytes, need);
   if ((reinterpret_cast<uintptr_t>(d_table) | reinterpret_cast<uintptr_t>(d_ws) |
        reinterpret_cast<uintptr_t>(d_plan)) & 255)
     return fail(FE_ERR_ARG, "fe_table_build: buffers must be 256-byte aligned");
@@ -438,6 +445,17 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
   a.keep = reinterpret_cast<int*>(wb + p->ws_keep);
   a.srule = reinterpret_cast<double*>(wb + p->ws_srule);
   a.swork = reinterpret_cast<int*>(wb + p->ws_swork);
+  a.nbox = (n_pts + 31) / 32;
+  a.nsbox = (a.nbox + 31) / 32;
+  double* box = reinterpret_cast<double*>(wb + p->ws_bytes);
+  double* sbox = reinterpret_cast<double*>(wb + p->ws_bytes + align256(size_t(a.nbox) * 6 * sizeof(double)));
+  a.box = box;
+  a.sbox = sbox;
+  if (a.nbox > 0) {
+    fe_point_boxes_kernel<<<(a.nbox + 127) / 128, 128, 0, st>>>(d_pts, n_pts, box, a.nbox);
+    fe_super_boxes_kernel<<<(a.nsbox + 127) / 128, 128, 0, st>>>(box, a.nbox, sbox, a.nsbox);
+    FE_CUDA(cudaGetLastError());
+  }
   if (p->nblocks > 0) {
     fe_build_kernel<<<p->nblocks, FE_BUILD_THREADS, 0, st>>>(a);
     FE_CUDA(cudaGetLastError());

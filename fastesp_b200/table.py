@@ -521,7 +521,7 @@ def build_table(wfn: Wavefunction, basis: Basis, density, points, tol: float = 1
         raise ValueError(f"density must be ({basis.n}, {basis.n}), got {tuple(dens.shape)}")
     pts_d = _to_dev(points, dev).reshape(-1, 3)
     buf = _empty_bytes(plan.sizes.table_bytes, dev)
-    ws = _empty_bytes(plan.sizes.build_ws_bytes, dev)
+    ws = _empty_bytes(_lib.lib().fe_build_ws_bytes(plan._h, int(pts_d.shape[0])), dev)
     _lib.check(_lib.lib().fe_table_build(plan._h, _lib.ptr(plan.d_plan), _lib.ptr(dens),
                                          _lib.ptr(pts_d), int(pts_d.shape[0]), float(tol),
                                          _lib.RULES[rule], _lib.ptr(buf), _lib.ptr(ws),

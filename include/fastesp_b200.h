@@ -57,7 +57,7 @@ typedef struct fe_plan fe_plan;    /* opaque, host memory */
 typedef struct fe_sizes {
   size_t plan_bytes;       /* device bytes of the uploaded plan */
   size_t table_bytes;      /* device bytes of one pair table */
-  size_t build_ws_bytes;   /* device workspace of fe_table_build */
+  size_t build_ws_bytes;   /* device workspace of fe_table_build without points (fe_build_ws_bytes) */
   int n_shell, n_shell_pair, n_work;
   int cap[FE_NCLASS];      /* primitive-pair slots per class (upper bound of kept pairs) */
 } fe_sizes;
@@ -93,6 +93,10 @@ int fe_plan_sizes(const fe_plan* plan, fe_sizes* sizes);
 
 /* Copy the plan to the caller's device buffer (plan_bytes, 256-byte aligned). */
 int fe_plan_upload(const fe_plan* plan, void* d_plan, cudaStream_t stream);
+
+/* Workspace bytes of fe_table_build with n_pts screening points: the plan's
+ * build_ws_bytes plus the bounding boxes of the point blocks. */
+size_t fe_build_ws_bytes(const fe_plan* plan, int n_pts);
 
 /* Build the pair table on the GPU: E-coefficients, density-weighted Hermite
  * table, G[alpha, m] contraction, screening bound and point screen, then an
