@@ -312,6 +312,8 @@ def run_ours(args):
         "published_reference": PUBLISHED,
     }
     line["clocks"] = clk.summary()
+    if world == 1 and not args.no_extras:
+        line["extras"] = run_extras(args, dev, flush)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wfn, basis, P, pts, counts, budget_s=args.cpu_budget)
     if world > 1:
@@ -319,6 +321,93 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# the other workloads: grid sweep, adjoint, batch (reported beside the headline)
+# ---------------------------------------------------------------------------
+def _median_ms(fn, reps, warm=2, flush=None):
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        if flush is not None:
+            flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        b.synchronize()
+        ts.append(a.elapsed_time(b))
+    return statistics.median(ts)
+
+
+def run_extras(args, dev, flush):
+    """Grid sweep (mixed vs FP64 on a cubic grid), the adjoint on the 20-atom
+    l<=2 system, and the 64-molecule batch against 64 plain launches."""
+    import torch
+    from fastesp_b200 import build_table, synth
+    from fastesp_b200.batch import BatchESP, separate_launches
+    out = {}
+    wfn, basis, P, _ = synth.load_workload("frag54", 10, seed=0)
+    P_d = torch.as_tensor(P, device=dev)
+    sweep = []
+    for n in args.grid_points:
+        pts = torch.as_tensor(synth.cubic_grid_points(wfn.coords, n, seed=2), device=dev)
+        tb = _median_ms(lambda: build_table(wfn, basis, P_d, pts), 3, warm=1, flush=flush)
+        tab = build_table(wfn, basis, P_d, pts)
+        v64 = tab.esp(pts)
+        vmx, n64 = tab.esp_stats(pts)
+        d = (vmx - v64).abs()
+        t64 = _median_ms(lambda: tab.esp(pts), 3, warm=1, flush=flush)
+        tmx = _median_ms(lambda: tab.esp(pts, precision="mixed"), 3, warm=1, flush=flush)
+        sweep.append({"points": int(pts.shape[0]), "pairs": tab.n_pairs, "build_ms": tb,
+                      "fp64_ms": t64, "mixed_ms": tmx, "mixed_over_fp64": t64 / tmx,
+                      "fp64_points_per_s": pts.shape[0] / (t64 * 1e-3),
+                      "mixed_points_per_s": pts.shape[0] / (tmx * 1e-3),
+                      "mixed_max_abs_err": float(d.max()), "mixed_rms_err": float(d.pow(2).mean().sqrt()),
+                      "fp64_routed_pair_warp_evals": n64})
+        del tab, pts, v64, vmx
+    out["grid_sweep"] = {"workload": "frag54 on a cubic grid of 0.2 Bohr spacing, 4 Bohr margin, "
+                                     "points within 0.3 Bohr of a nucleus dropped; errors of the "
+                                     "mixed path against the FP64 path", "runs": sweep}
+    # adjoint: 20 atoms l<=2, 500 surface points, L = 0.5 ||V - V_target||^2
+    w3, b3, P3, p3 = synth.load_workload("adjoint20", 500, seed=0)
+    P3d = torch.as_tensor(P3, device=dev)
+    p3d = torch.as_tensor(p3, device=dev)
+    rng = np.random.default_rng(7)
+    E = rng.normal(0.0, 1e-3, P3.shape)
+    vt = build_table(w3, b3, P3d + torch.as_tensor(0.5 * (E + E.T), device=dev), p3d).esp(p3d)
+    t3 = build_table(w3, b3, P3d, p3d)
+    wv = t3.esp(p3d) - vt
+    t_fwd = _median_ms(lambda: build_table(w3, b3, P3d, p3d).esp(p3d), 5)
+    t_adj = _median_ms(lambda: t3.adjoint(p3d, wv), 5)
+    t_fld = _median_ms(lambda: t3.adjoint(p3d, wv, density=False), 5)
+    out["adjoint"] = {"workload": f"adjoint20: 20 atoms, l<=2, {b3.n} Cartesian functions, 500 points",
+                      "pairs": t3.n_pairs, "forward_ms": t_fwd, "adjoint_dP_dC_ms": t_adj,
+                      "adjoint_dC_only_ms": t_fld}
+    # batch: 64 uneven molecules
+    mols = synth.batch_workload(64, seed=0)
+    tabs, pts = [], []
+    for wfn_, basis_, P_, p_ in mols:
+        pd = torch.as_tensor(p_, device=dev)
+        tabs.append(build_table(wfn_, basis_, torch.as_tensor(P_, device=dev), pd))
+        pts.append(pd)
+    b = BatchESP(tabs, pts)
+    _, run_sep = separate_launches(tabs, pts)
+    tbat = _median_ms(b.run, 10, flush=flush)
+    tsep = _median_ms(run_sep, 10, flush=flush)
+    err = max(float((x - y).abs().max()) for x, y in zip(b.run(), run_sep()))
+    npts = sum(int(p.shape[0]) for p in pts)
+    out["batch"] = {"workload": "64 molecules, 5-60 atoms, l<=2, 200-5000 surface points each",
+                    "points": npts, "pairs": sum(t.n_pairs for t in tabs),
+                    "batched_graph_ms": tbat, "separate_launches_ms": tsep,
+                    "speedup": tsep / tbat, "points_per_s": npts / (tbat * 1e-3),
+                    "shape": list(b.shape), "items": b.n_items, "max_abs_diff": err,
+                    "autotune_ms": {f"{k[0]}x{k[1]}": v for k, v in (b.tuning or {}).items()}}
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -414,6 +503,9 @@ def main():
     ap.add_argument("--points", type=int, default=30000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the grid sweep, adjoint and batch measurements")
+    ap.add_argument("--grid-points", type=int, nargs="*", default=[100000, 1000000])
     ap.add_argument("--eval-only", action="store_true",
                     help="time only the two evaluators (short run for profiling)")
     args = ap.parse_args()

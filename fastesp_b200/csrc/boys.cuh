@@ -110,3 +110,51 @@ FE_DEV void fe_boys_f32(const float T, const float rt, const float* __restrict__
     for (int m = M; m > 0; --m) F[m - 1] = fmaf(t2, F[m], e) * (1.0f / float(2 * m - 1));
   }
 }
+
+// Packed FP32 Boys vectors of two arguments (one per float2 lane), for the
+// orders whose FP32 asymptotic threshold lies below the grid's end (M <= 6):
+// the tabulated and the asymptotic branch only.  Each lane gets what
+// fe_boys_f32 gives it (the same operations lane by lane); when the lanes fall
+// in different branches both are computed and each lane keeps its own.
+template <int M>
+FE_DEV void fe_boys_f32x2(const float2 T, const float2 rt, const float* __restrict__ grid,
+                          float2 (&F)[M + 1]) {
+  constexpr float t_asym = fe_boys32_asym_T[M];
+  static_assert(fe_boys32_asym_T[M] <= FE_BOYS32_GRID_TMAX, "two-branch form only");
+  const bool ax = T.x >= t_asym, ay = T.y >= t_asym;
+  float2 A[M + 1], G[M + 1];
+  if (ax || ay) {
+    const float2 h = fe_f2(0.5f) * rt * rt;
+    A[0] = fe_f2(float(FE_SQRT_PI_2)) * rt;
+#pragma unroll
+    for (int m = 0; m < M; ++m) A[m + 1] = A[m] * (fe_f2(float(2 * m + 1)) * h);
+  }
+  if (!(ax && ay)) {
+    // a lane in the asymptotic range reads a clamped, in-range row; its result is dropped
+    const float2 ti = T * fe_f2(FE_BOYS32_GRID_INV_H);
+    const int ix = min(max(__float2int_rn(ti.x), 0), FE_BOYS32_NROW - 1);
+    const int iy = min(max(__float2int_rn(ti.y), 0), FE_BOYS32_NROW - 1);
+    const float2 d = make_float2(float(ix), float(iy)) * fe_f2(FE_BOYS32_GRID_H) - T;   // exact
+    const float* rx = grid + ix * FE_BOYS32_NTAB + M;
+    const float* ry = grid + iy * FE_BOYS32_NTAB + M;
+    float2 f = make_float2(rx[FE_BOYS32_TAYLOR_K - 1], ry[FE_BOYS32_TAYLOR_K - 1]);
+#pragma unroll
+    for (int k = FE_BOYS32_TAYLOR_K - 2; k >= 0; --k)
+      f = fe_fma(f, d * fe_f2(1.0f / float(k + 1)), make_float2(rx[k], ry[k]));
+    G[M] = f;
+    const float2 e = make_float2(__expf(-T.x), __expf(-T.y));
+    const float2 t2 = T + T;
+#pragma unroll
+    for (int m = M; m > 0; --m) G[m - 1] = fe_fma(t2, G[m], e) * fe_f2(1.0f / float(2 * m - 1));
+  }
+  if (ax && ay) {
+#pragma unroll
+    for (int m = 0; m <= M; ++m) F[m] = A[m];
+  } else if (!ax && !ay) {
+#pragma unroll
+    for (int m = 0; m <= M; ++m) F[m] = G[m];
+  } else {
+#pragma unroll
+    for (int m = 0; m <= M; ++m) F[m] = make_float2(ax ? A[m].x : G[m].x, ay ? A[m].y : G[m].y);
+  }
+}

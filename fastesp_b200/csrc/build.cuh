@@ -531,7 +531,7 @@ __global__ void fe_make_f32_kernel(unsigned char* table) {
     split(r[4], o[8], o[9]);
     o[10] = float(r[5]);                 // K * bound (+inf when unknown)
     o[11] = float(1.0 / sqrt(r[0]));     // p^-1/2
-    for (int k = 0; k < NT; ++k) split(r[6 + k], o[12 + k], o[12 + NT + k]);
+    for (int k = 0; k < NT; ++k) o[12 + 2 * k] = o[13 + 2 * k] = float(r[6 + k]);
     for (int k = 12 + 2 * NT; k < R32; ++k) o[k] = 0.0f;
   }
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) hdr->has32 = 1;

@@ -17,6 +17,16 @@ FE_DEV void fe_flag(unsigned bits) { atomicOr(&fe_status_word, bits); }
 FE_DEV double fe_fma(double a, double b, double c) { return fma(a, b, c); }
 FE_DEV float fe_fma(float a, float b, float c) { return fmaf(a, b, c); }
 
+// Packed FP32x2 arithmetic (two lanes per instruction on sm_100), round to
+// nearest, no contraction beyond the explicit fused multiply-add: the same
+// results as the scalar operations lane by lane.
+FE_DEV float2 fe_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+FE_DEV float2 operator*(float2 a, float2 b) { return __fmul2_rn(a, b); }
+FE_DEV float2& operator*=(float2& a, float2 b) { a = __fmul2_rn(a, b); return a; }
+FE_DEV float2 operator+(float2 a, float2 b) { return __fadd2_rn(a, b); }
+FE_DEV float2 operator-(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+FE_DEV float2 fe_f2(float v) { return make_float2(v, v); }
+
 FE_DEV unsigned smem_u32(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }

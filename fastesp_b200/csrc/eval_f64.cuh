@@ -4,9 +4,10 @@
 // (fastesp/native/esp_gpu.cu:161-229) and PairTable.electron/esp
 // (fastesp/table.py:73-104).
 //
-// Grid (x = point block, y = pair split).  A block owns FE_EVAL_THREADS * NP
-// points (NP per thread, kept in registers) and 1/nsplit of the pairs of every
-// class.  Its pairs are walked as tiles of whole records; thread 0 streams the
+// Grid (x = point block, y = pair rows).  A block owns FE_EVAL_THREADS * NP
+// points (NP per thread, kept in registers) and, through fe_class_rows, one
+// part of one class's pairs (rows class-major, so concurrently running blocks
+// execute the same class's code).  Its pairs are walked as tiles of whole records; thread 0 streams the
 // tiles into a FE_NSTAGE-deep ring of shared-memory stages with 1-D TMA bulk
 // copies completing on per-stage mbarriers, and every thread reads the current
 // record as a warp-uniform broadcast, so each coefficient load feeds NP fused
@@ -77,6 +78,39 @@ FE_DEV void fe_block_work(const FeTableHdr* hdr, int split, int nsplit, const in
   }
   w.total = total;
   w.wtotal = words;
+}
+
+// Class-major assignment of a kernel's ``Y`` grid rows to the classes
+// [llo, hi] that hold pairs: class L gets 1 + floor((Y - nz) W_L / sum W) rows
+// (nz: classes with pairs; W_L = its 32-pair words times a per-pair cost),
+// rows in class order, leftover rows idle (L = -1).  Row y -> (class L, part s
+// of nL).  Blocks with consecutive y run the same class's code, so the SMs
+// share one class's instructions at a time.  Needs Y >= nz.
+FE_DEV void fe_class_rows(const FeTableHdr* hdr, int llo, int lhi, int Y, int y, int& L,
+                          int& s, int& nL) {
+  double W[FE_NCLASS], sum = 0.0;
+  int nz = 0;
+  for (int l = 0; l < FE_NCLASS; ++l) {
+    const int words = (l >= llo && l <= lhi) ? (hdr->count[l] + 31) / 32 : 0;
+    W[l] = double(words) * (2.0 * fe_c_nterm[l] + 20.0);
+    sum += W[l];
+    nz += words > 0;
+  }
+  int row = 0;
+  for (int l = 0; l < FE_NCLASS; ++l) {
+    if (W[l] == 0.0) continue;
+    const int n = 1 + int(double(Y - nz) * W[l] / sum);
+    if (y < row + n) {
+      L = l;
+      s = y - row;
+      nL = n;
+      return;
+    }
+    row += n;
+  }
+  L = -1;
+  s = 0;
+  nL = 1;
 }
 
 // Tile i of the block -> (class, first pair, pair count).
@@ -219,7 +253,10 @@ __global__ void __launch_bounds__(NT, MINB) fe_eval_f64_kernel(const FeEvalArgs 
     acc[j] = 0.0;
   }
   FeTilePipe pipe{a.table, fe_c_tile64, fe_c_rec64, hdr->off64, 8, fe_smem, full_bar, &w};
-  pipe.start(hdr, split, a.nsplit, LLO, LHI);
+  int Lrow, part, nparts;
+  fe_class_rows(hdr, LLO, LHI, a.nsplit, split, Lrow, part, nparts);
+  if (Lrow >= 0) pipe.start(hdr, part, nparts, Lrow, Lrow);
+  else pipe.start(hdr, 0, 1, 1, 0);                     // idle row: no tiles
   const int total = w.total;
   for (int i = 0; i < total; ++i) {
     if (!pipe.wait(i)) {

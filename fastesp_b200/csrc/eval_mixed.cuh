@@ -184,6 +184,70 @@ FE_DEV void fe_tile_f32(const float* __restrict__ rec, int first, int n, int hi,
   }
 }
 
+// The same routing test and FP32 evaluation with two points per float2 lane
+// (packed FP32x2 instructions; point 2q + e of the thread in lane e of q).
+// Lane by lane the operations are those of fe_route / fe_tile_f32, so the
+// results are the same bit for bit.
+FE_DEV void fe_two_sum2(float2& hi, float2& lo, float2 b) {
+  const float2 s = hi + b;
+  const float2 bb = s - hi;
+  const float2 err = (hi - (s - bb)) + (b - bb);
+  hi = s;
+  lo = lo + err;
+}
+
+template <int NQ>
+FE_DEV bool fe_route2(const float* __restrict__ rec, const float2 (&cxh)[NQ],
+                      const float2 (&cyh)[NQ], const float2 (&czh)[NQ], const float2 (&cxl)[NQ],
+                      const float2 (&cyl)[NQ], const float2 (&czl)[NQ], float2 (&x)[NQ],
+                      float2 (&y)[NQ], float2 (&z)[NQ], float2 (&r2)[NQ], float2 (&ir)[NQ],
+                      float tau) {
+  const float kb = rec[10];
+  const float2 pxh = fe_f2(rec[2]), pyh = fe_f2(rec[3]), pzh = fe_f2(rec[4]);
+  const float2 pxl = fe_f2(rec[5]), pyl = fe_f2(rec[6]), pzl = fe_f2(rec[7]);
+  bool need = false;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    x[q] = (cxh[q] - pxh) + (cxl[q] - pxl);
+    y[q] = (cyh[q] - pyh) + (cyl[q] - pyl);
+    z[q] = (czh[q] - pzh) + (czl[q] - pzl);
+    r2[q] = fe_fma(x[q], x[q], fe_fma(y[q], y[q], z[q] * z[q]));
+    ir[q] = make_float2(rsqrtf(r2[q].x), rsqrtf(r2[q].y));
+    need |= !(__fmul_rn(kb, ir[q].x) < tau) || !(__fmul_rn(kb, ir[q].y) < tau);
+  }
+  return __any_sync(0xffffffffu, need);
+}
+
+template <int L, int NQ>
+FE_DEV void fe_tile_f32x2(const float* __restrict__ rec, int first, int n, int hi,
+                          const float2 (&cxh)[NQ], const float2 (&cyh)[NQ],
+                          const float2 (&czh)[NQ], const float2 (&cxl)[NQ],
+                          const float2 (&cyl)[NQ], const float2 (&czl)[NQ], float2 (&ahi)[NQ],
+                          float2 (&alo)[NQ], const float* __restrict__ grid, float tau,
+                          unsigned* __restrict__ mw, unsigned& bits) {
+  constexpr int S32 = fe_class_rec32[L];
+  const bool lane0 = (threadIdx.x & 31) == 0;
+#pragma unroll 1
+  for (int i = 0; i < n; ++i, rec += S32) {
+    const int gi = first + i;
+    float2 x[NQ], y[NQ], z[NQ], r2[NQ], ir[NQ];
+    const bool routed = fe_route2<NQ>(rec, cxh, cyh, czh, cxl, cyl, czl, x, y, z, r2, ir, tau);
+    bits |= unsigned(routed) << (gi & 31);
+    if ((gi & 31) == 31 || gi + 1 == hi) {
+      if (lane0 && mw) mw[gi >> 5] = bits;
+      bits = 0u;
+    }
+    if (routed) continue;
+    const float2 pe = fe_f2(rec[0]), rsp = fe_f2(rec[11]), K = fe_f2(rec[8]);
+    float2 F[NQ][L + 1], s[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) fe_boys_f32x2<L>(pe * r2[q], ir[q] * rsp, grid, F[q]);
+    fe_poly32x2<L, NQ>(rec + 12, x, y, z, F, s);
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) fe_two_sum2(ahi[q], alo[q], K * s[q]);
+  }
+}
+
 // FP64 evaluation of one routed pair (record ``rec64`` in shared memory) for
 // this thread's points, two at a time for instruction-level parallelism.
 template <int L, int NP>
@@ -224,6 +288,10 @@ FE_DEV void fe_pair_fix64(const double* __restrict__ rec64, const double (&cx)[N
 template <int MINB, int LLO, int LHI>
 __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMixedArgs a) {
   constexpr int NP = FE_MX_NP, NT = FE_MX_NT;
+  // classes up to 6 run packed (two points per float2 lane); the g-shell
+  // classes, whose FP32 Boys vector also has the erf branch, run scalar
+  constexpr bool PACKED = LHI <= 6 && NP % 2 == 0;
+  constexpr int NQ = NP / 2;
   extern __shared__ __align__(128) unsigned char fe_smem[];
   __shared__ uint64_t full_bar[FE_NSTAGE];
   __shared__ FeBlockWork w;
@@ -236,8 +304,22 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
   fe_load_points_split<NP>(a.pts, a.npts, p0, NT, cxh, cyh, czh, cxl, cyl, czl);
 #pragma unroll
   for (int j = 0; j < NP; ++j) ahi[j] = alo[j] = 0.0f;
+  float2 cxh2[NQ], cyh2[NQ], czh2[NQ], cxl2[NQ], cyl2[NQ], czl2[NQ], ahi2[NQ], alo2[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    cxh2[q] = make_float2(cxh[2 * q], cxh[2 * q + 1]);
+    cyh2[q] = make_float2(cyh[2 * q], cyh[2 * q + 1]);
+    czh2[q] = make_float2(czh[2 * q], czh[2 * q + 1]);
+    cxl2[q] = make_float2(cxl[2 * q], cxl[2 * q + 1]);
+    cyl2[q] = make_float2(cyl[2 * q], cyl[2 * q + 1]);
+    czl2[q] = make_float2(czl[2 * q], czl[2 * q + 1]);
+    ahi2[q] = alo2[q] = make_float2(0.0f, 0.0f);
+  }
   FeTilePipe pipe{a.table, fe_c_tile32, fe_c_rec32, hdr->off32, 4, fe_smem, full_bar, &w};
-  pipe.start(hdr, blockIdx.y, a.nsplit, LLO, LHI, 32);
+  int Lrow, part, nparts;
+  fe_class_rows(hdr, LLO, LHI, a.nsplit, blockIdx.y, Lrow, part, nparts);
+  if (Lrow >= 0) pipe.start(hdr, part, nparts, Lrow, Lrow, 32);
+  else pipe.start(hdr, 0, 1, 1, 0, 32);                 // idle row: no tiles
   const int total = w.total;
   const long long warp_g = (long long)blockIdx.x * (NT / 32) + (tid >> 5);
   unsigned* mrow = a.mask + warp_g * w.wtotal;
@@ -255,11 +337,27 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
     fe_item(w, fe_c_tile32, i, L, first, n);
     const float* rec = reinterpret_cast<const float*>(pipe.stage(i));
     unsigned* mw = mrow ? mrow + w.woff[L] : nullptr;
+    if constexpr (PACKED) {
+#define FE_CALL32(l) fe_tile_f32x2<l, NQ>(rec, first, n, w.hi[L], cxh2, cyh2, czh2, cxl2, cyl2, \
+                                          czl2, ahi2, alo2, grid, a.tau, mw, bits)
+      FE_MX_SWITCH(FE_CALL32)
+#undef FE_CALL32
+    } else {
 #define FE_CALL32(l) fe_tile_f32<l, NP>(rec, first, n, w.hi[L], cxh, cyh, czh, cxl, cyl, czl, \
                                         ahi, alo, grid, a.tau, mw, bits)
-    FE_MX_SWITCH(FE_CALL32)
+      FE_MX_SWITCH(FE_CALL32)
 #undef FE_CALL32
+    }
     pipe.release(i);
+  }
+  if constexpr (PACKED) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      ahi[2 * q] = ahi2[q].x;
+      ahi[2 * q + 1] = ahi2[q].y;
+      alo[2 * q] = alo2[q].x;
+      alo[2 * q + 1] = alo2[q].y;
+    }
   }
 #pragma unroll
   for (int j = 0; j < NP; ++j) {
@@ -268,11 +366,12 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
   }
 }
 
-// The FP64 part: every warp walks its row of the routing mask over its split's
-// share of the words of each class; for each set bit it copies that pair's
-// FP64 record into a per-warp shared buffer and evaluates it for its points.
-// Pairs are visited in class order, then pair order, so the sum is
-// deterministic.
+// The FP64 part: grid row y takes one class and a part of its mask words
+// (fe_class_rows, class-major so that concurrently running blocks execute
+// the same class's code); every warp walks its row of the routing mask over
+// those words and, for each set bit, copies that pair's FP64 record into a
+// per-warp shared buffer and evaluates it for its points.  Each grid row
+// writes its own partial sums, so the result is deterministic.
 #define FE_FIX_BUF 320      // doubles per warp buffer (class-8 record: 300)
 
 template <int MINB, int LLO, int LHI>
@@ -301,10 +400,12 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_fix64_kernel(const FeM
   unsigned n64 = 0;
   if ((warp_g + 1) * w.wtotal <= a.mask_words) {
     const unsigned* mrow = a.mask + warp_g * w.wtotal;
-    for (int L = LLO; L <= LHI; ++L) {
+    int L, part, nparts;
+    fe_class_rows(hdr, LLO, LHI, a.nsplit, blockIdx.y, L, part, nparts);
+    if (L >= 0) {
       const int nw = (hdr->count[L] + 31) / 32;
-      const int w0 = int((long long)nw * blockIdx.y / a.nsplit);
-      const int w1 = int((long long)nw * (blockIdx.y + 1) / a.nsplit);
+      const int w0 = int((long long)nw * part / nparts);
+      const int w1 = int((long long)nw * (part + 1) / nparts);
       const int S64 = fe_c_rec64[L];
       const double* base = reinterpret_cast<const double*>(a.table + hdr->off64[L]);
       for (int c = w0; c < w1; c += 32) {

@@ -70,7 +70,7 @@ int sm_count() {
 #define FE_MINB64 3
 #endif
 #ifndef FE_MINB32
-#define FE_MINB32 4
+#define FE_MINB32 3
 #endif
 #ifndef FE_MINBFIX
 #define FE_MINBFIX 4
@@ -110,16 +110,18 @@ EvalGeom eval_geom(int npts, int mode) {
   };
   const int hi_splits = std::max(1, std::min(8, sm_count() / std::max(1, g.nblk_x)));
   g.ld = (npts + 31) & ~31;
+  // every kernel needs at least one grid row per class of its range (fe_class_rows)
+  const int nlo = FE_LSPLIT + 1, nhi = FE_NCLASS - 1 - FE_LSPLIT;
   if (mode == 1) {
     g.nkern = 4;
-    g.split[0] = splits(kMinB32);
-    g.split[1] = hi_splits;
-    g.split[2] = splits(kMinBFix);
-    g.split[3] = hi_splits;
+    g.split[0] = std::max(nlo, splits(kMinB32));
+    g.split[1] = std::max(nhi, hi_splits);
+    g.split[2] = std::max(nlo, splits(kMinBFix));
+    g.split[3] = std::max(nhi, hi_splits);
   } else {
     g.nkern = 2;
-    g.split[0] = splits(kMinB64);
-    g.split[1] = hi_splits;
+    g.split[0] = std::max(nlo, splits(kMinB64));
+    g.split[1] = std::max(nhi, hi_splits);
   }
   return g;
 }

@@ -101,12 +101,13 @@ class CoefLoader:
     per ``vec`` consecutive coefficients (float4 / double2), 0 scalar loads.
     """
 
-    def __init__(self, em, order=None, vec=0, vtype=""):
+    def __init__(self, em, order=None, vec=0, vtype="", dup=None):
         self.em = em
         self.pos = {} if order is None else {k: i for i, k in enumerate(order)}
         self.fixed = order is not None
         self.vec = vec
         self.vtype = vtype
+        self.dup = dup          # None, "scalar" or "packed": FP32 {g, g} pairs
         self.loaded = set()
 
     def expr(self, k):
@@ -114,6 +115,15 @@ class CoefLoader:
             assert not self.fixed
             self.pos[k] = len(self.pos)
         p = self.pos[k]
+        if self.dup:
+            # coefficient p occupies floats 2p, 2p+1 (the same value twice), so one
+            # float4 holds two coefficients, each already a float2 pair
+            c, half = divmod(p, 2)
+            if c not in self.loaded:
+                self.loaded.add(c)
+                self.em.w(f"const float4 gv{c} = *reinterpret_cast<const float4*>(g + {4 * c});")
+            a, b = ("x", "y") if half == 0 else ("z", "w")
+            return f"make_float2(gv{c}.{a}, gv{c}.{b})" if self.dup == "packed" else f"gv{c}.{a}"
         if not self.vec:
             return f"g[{p}]"
         c, lane = divmod(p, self.vec)
@@ -126,10 +136,10 @@ class CoefLoader:
         return [k for k, _ in sorted(self.pos.items(), key=lambda kv: kv[1])]
 
 
-def poly_m_major(L, order=None, vec=0, vtype=""):
+def poly_m_major(L, order=None, vec=0, vtype="", dup=None):
     keys, _ = H.class_terms(L)
     em = Emitter()
-    ld = CoefLoader(em, order, vec, vtype)
+    ld = CoefLoader(em, order, vec, vtype, dup)
     by_m = {}
     for k, (ax, ay, az, m) in enumerate(keys):
         by_m.setdefault(m, {})[(ax, ay, az)] = k
@@ -146,10 +156,10 @@ def poly_m_major(L, order=None, vec=0, vtype=""):
     return em, ld
 
 
-def poly_alpha_major(L, order=None, vec=0, vtype=""):
+def poly_alpha_major(L, order=None, vec=0, vtype="", dup=None):
     keys, _ = H.class_terms(L)
     em = Emitter()
-    ld = CoefLoader(em, order, vec, vtype)
+    ld = CoefLoader(em, order, vec, vtype, dup)
     by_a = {}
     for k, (ax, ay, az, m) in enumerate(keys):
         by_a.setdefault((ax, ay, az), []).append((k, m))
@@ -186,15 +196,22 @@ def consumption_order(L):
 
 
 def poly_functions(L):
+    """FP32 (coefficients stored as {g, g} pairs), packed FP32x2 (two points per
+    float2, the same pairs as operands) and FP64 (double2 loads) evaluators."""
     build, tag, nops = poly_variant(L)
     order = consumption_order(L)
     out = []
-    for real, vtype, vec, suffix in (("float", "float4", 4, "32"), ("double", "double2", 2, "64")):
-        em, _ = build(L, order, vec, vtype)
+    for real, vtype, vec, suffix, dup in (("float", "float4", 4, "32", "scalar"),
+                                          ("float2", "float4", 4, "32x2", "packed"),
+                                          ("double", "double2", 2, "64", None)):
+        em, _ = build(L, order, vec, vtype, dup)
+        lay = ("coefficients g[2k] = g[2k+1] = G_k in consumption order" if dup else
+               "coefficients g[k] in consumption order")
         out += [f"// class L={L}: {H.n_terms(L)} terms, {nops} fused ops per point ({tag}),",
-                f"// coefficients g[0..{H.n_terms(L)}) in consumption order, 16-byte aligned",
+                f"// {lay}, 16-byte aligned"
+                + ("; two points per float2 lane" if dup == "packed" else ""),
                 "template <int NP>",
-                f"__device__ __forceinline__ void fe_poly{suffix}_L{L}(const {real}* __restrict__ g,",
+                f"__device__ __forceinline__ void fe_poly{suffix}_L{L}(const {'float' if dup else real}* __restrict__ g,",
                 f"    const {real} (&x)[NP], const {real} (&y)[NP], const {real} (&z)[NP],",
                 f"    const {real} (&F)[NP][{L + 1}], {real} (&s)[NP]) {{",
                 "  using Real = " + real + ";",
@@ -484,6 +501,16 @@ def main() -> int:
         out.append(f"    if constexpr (sizeof(Real) == 4) fe_poly32_L{L}<NP>(g, x, y, z, F, s);")
         out.append(f"    else fe_poly64_L{L}<NP>(g, x, y, z, F, s);")
         out.append("  }")
+    out.append("}")
+    out.append("")
+    out.append("// the same for two points per float2 lane (FP32 records, {g, g} coefficient pairs)")
+    out.append("template <int L, int NP>")
+    out.append("__device__ __forceinline__ void fe_poly32x2(const float* __restrict__ g,")
+    out.append("    const float2 (&x)[NP], const float2 (&y)[NP], const float2 (&z)[NP],")
+    out.append("    const float2 (&F)[NP][L + 1], float2 (&s)[NP]) {")
+    for L in range(LMAX + 1):
+        kw = "if" if L == 0 else "else if"
+        out.append(f"  {kw} constexpr (L == {L}) fe_poly32x2_L{L}<NP>(g, x, y, z, F, s);")
     out.append("}")
     out.append("")
     out.append("template <int L, typename Real, int NP>")

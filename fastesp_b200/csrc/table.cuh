@@ -15,10 +15,13 @@
 // the reference builder: shell pairs (si <= sj) in shell order, then
 // primitive pairs with the primitive of shell si outer.
 //
-// Mixed-precision records are fe_class_rec32[L] floats holding every FP64 value
-// v as hi = float(v), lo = float(v - hi):
+// Mixed-precision records are fe_class_rec32[L] floats: the pair's scalars as
+// hi = float(v), lo = float(v - hi) splits, then every coefficient twice, so
+// a 16-byte load yields two coefficients each already a {g, g} operand pair
+// of the packed FP32x2 arithmetic:
 // [p_hi, p_lo, Px_hi, Py_hi, Pz_hi, Px_lo, Py_lo, Pz_lo, K_hi, K_lo, K*bound,
-//  p^-1/2, G_hi[0..nt), G_lo[0..nt), pad to 16 bytes].
+//  p^-1/2, G_0, G_0, G_1, G_1, ..., G_(nt-1), G_(nt-1), pad to 16 bytes]
+// (G in the same consumption order as the FP64 record).
 //
 // The source section maps every record of a table built on the device back to
 // the builder's work item (shell pair and primitive indices), so the adjoint

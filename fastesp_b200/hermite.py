@@ -105,11 +105,10 @@ def record_stride(L: int) -> int:
 def record_stride_f32(L: int) -> int:
     """FP32 words per mixed-precision record, padded to 16 bytes.
 
-    Every FP64 value v of the FP64 record is kept as a float pair
-    hi = float(v), lo = float(v - hi) (hi + lo carries ~48 bits of v):
+    The pair's scalars as float pairs hi = float(v), lo = float(v - hi), then
+    every coefficient twice (a {g, g} operand pair of the packed FP32x2 code):
     [p_hi, p_lo, Px_hi, Py_hi, Pz_hi, Px_lo, Py_lo, Pz_lo, K_hi, K_lo, K*bound,
-    p^-1/2, G_hi[0..nt), G_lo[0..nt)].  The FP32 path reads the hi halves; the
-    FP64 fallback rebuilds the FP64 values from both halves.
+    p^-1/2, G_0, G_0, G_1, G_1, ...].
     """
     n = 12 + 2 * n_terms(L)
     return (n + 3) // 4 * 4
