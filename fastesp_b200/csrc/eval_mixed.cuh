@@ -189,11 +189,18 @@ FE_DEV void fe_tile_f32(const float* __restrict__ rec, int first, int n, int hi,
 // Lane by lane the operations are those of fe_route / fe_tile_f32, so the
 // results are the same bit for bit.
 FE_DEV void fe_two_sum2(float2& hi, float2& lo, float2 b) {
+#ifdef FE_FAST2SUM
+  const float2 s = hi + b;
+  const float2 err = b - (s - hi);
+  hi = s;
+  lo = lo + err;
+#else
   const float2 s = hi + b;
   const float2 bb = s - hi;
   const float2 err = (hi - (s - bb)) + (b - bb);
   hi = s;
   lo = lo + err;
+#endif
 }
 
 template <int NQ>

@@ -631,7 +631,7 @@ int eval_launch(const char* who, const void* d_table, const double* d_pts, int n
 }
 
 // Default FP64 routing threshold of the mixed evaluator (a.u.).
-constexpr double kTauDefault = 0.05;
+constexpr double kTauDefault = 0.1;
 
 }  // namespace
 
