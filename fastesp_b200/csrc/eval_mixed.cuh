@@ -374,17 +374,22 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
 }
 
 // The FP64 part: grid row y takes one class and a part of its mask words
-// (fe_class_rows, class-major so that concurrently running blocks execute
-// the same class's code); every warp walks its row of the routing mask over
-// those words and, for each set bit, copies that pair's FP64 record into a
-// per-warp shared buffer and evaluates it for its points.  Each grid row
-// writes its own partial sums, so the result is deterministic.
-#define FE_FIX_BUF 320      // doubles per warp buffer (class-8 record: 300)
+// (fe_class_rows, class-major so that concurrently running blocks execute the
+// same class's code).  The block walks its four warps' mask rows 32 words at a
+// time; for every word it takes the union of the warps' bits, copies the FP64
+// records of those pairs into shared memory in batches (all 128 threads), and
+// each warp then evaluates, for its points, the batch's pairs whose bit is set
+// in its own row.  Routed pairs are mostly routed for every warp, so a record
+// is fetched once per block instead of once per warp.  Every warp accumulates
+// its pairs in pair order and every grid row writes its own partial sums, so
+// the result is deterministic.
+#define FE_FIX_BUF 2304     // doubles of the record batch (16 class-6 records)
 
 template <int MINB, int LLO, int LHI>
 __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_fix64_kernel(const FeMixedArgs a) {
   constexpr int NP = FE_MX_NP, NT = FE_MX_NT, NW = FE_MX_NT / 32;
-  __shared__ __align__(16) double buf[NW][FE_FIX_BUF];
+  __shared__ __align__(16) double buf[FE_FIX_BUF];
+  __shared__ unsigned wb[NW][32];
   __shared__ FeBlockWork w;
   const FeTableHdr* hdr = reinterpret_cast<const FeTableHdr*>(a.table);
   const int tid = threadIdx.x, lane = tid & 31, wi = tid >> 5;
@@ -403,42 +408,65 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_fix64_kernel(const FeM
     fe_block_work(hdr, 0, 1, one, 0, FE_NCLASS - 1, w);    // word offsets only
   }
   __syncthreads();
-  const long long warp_g = (long long)blockIdx.x * NW + wi;
+  const long long warp0 = (long long)blockIdx.x * NW;
   unsigned n64 = 0;
-  if ((warp_g + 1) * w.wtotal <= a.mask_words) {
-    const unsigned* mrow = a.mask + warp_g * w.wtotal;
-    int L, part, nparts;
-    fe_class_rows(hdr, LLO, LHI, a.nsplit, blockIdx.y, L, part, nparts);
-    if (L >= 0) {
-      const int nw = (hdr->count[L] + 31) / 32;
-      const int w0 = int((long long)nw * part / nparts);
-      const int w1 = int((long long)nw * (part + 1) / nparts);
-      const int S64 = fe_c_rec64[L];
-      const double* base = reinterpret_cast<const double*>(a.table + hdr->off64[L]);
-      for (int c = w0; c < w1; c += 32) {
-        const unsigned word = c + lane < w1 ? mrow[w.woff[L] + c + lane] : 0u;
-        unsigned live = __ballot_sync(0xffffffffu, word != 0u);
-        while (live) {
-          const int src = __ffs(live) - 1;
-          live &= live - 1;
-          unsigned bitsw = __shfl_sync(0xffffffffu, word, src);
-          while (bitsw) {
-            const int b = __ffs(bitsw) - 1;
-            bitsw &= bitsw - 1;
-            const double* r = base + size_t((c + src) * 32 + b) * S64;
-            __syncwarp();
-            for (int k = lane; k < S64; k += 32) buf[wi][k] = __ldg(r + k);
-            __syncwarp();
+  int L, part, nparts;
+  fe_class_rows(hdr, LLO, LHI, a.nsplit, blockIdx.y, L, part, nparts);
+  if ((warp0 + NW) * w.wtotal > a.mask_words) {
+    if (tid == 0) fe_flag(FE_ST_OVERFLOW);
+    L = -1;
+  }
+  if (L >= 0) {
+    const int nw = (hdr->count[L] + 31) / 32;
+    const int w0 = int((long long)nw * part / nparts);
+    const int w1 = int((long long)nw * (part + 1) / nparts);
+    const int S64 = fe_c_rec64[L];
+    const int B = min(32, FE_FIX_BUF / S64);          // records per batch
+    const double* base = reinterpret_cast<const double*>(a.table + hdr->off64[L]);
+    const unsigned* mrow = a.mask + (warp0 + wi) * w.wtotal + w.woff[L];
+    for (int c0 = w0; c0 < w1; c0 += 32) {
+      __syncthreads();                                // wb and buf free
+      wb[wi][lane] = c0 + lane < w1 ? mrow[c0 + lane] : 0u;
+      __syncthreads();
+      const int kn = min(32, w1 - c0);
+      for (int k = 0; k < kn; ++k) {
+        unsigned rem = 0u;
+#pragma unroll
+        for (int v = 0; v < NW; ++v) rem |= wb[v][k];
+        const unsigned mine = wb[wi][k];
+        const size_t pair0 = size_t(c0 + k) * 32;
+        while (rem) {                                 // block-uniform
+          // the next batch: the lowest B set bits of rem
+          unsigned bm = 0u, r = rem;
+          for (int t = 0; t < B && r; ++t) {
+            bm |= r & (0u - r);
+            r &= r - 1;
+          }
+          rem = r;
+          const int nb = __popc(bm);
+          // copy: record t of the batch (its t-th set bit) by warp t % NW
+          for (int t = wi; t < nb; t += NW) {
+            unsigned r2 = bm;                         // its t-th set bit
+            for (int u = 0; u < t; ++u) r2 &= r2 - 1;
+            const int bit = __ffs(r2) - 1;
+            const double* src = base + (pair0 + bit) * S64;
+            for (int q = lane; q < S64; q += 32) buf[t * S64 + q] = __ldg(src + q);
+          }
+          __syncthreads();
+          unsigned todo = bm & mine;
+          while (todo) {                              // warp-uniform
+            const int bit = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int t = __popc(bm & ((1u << bit) - 1u));
             ++n64;
-#define FE_CALLP(l) fe_pair_fix64<l, NP>(buf[wi], cx, cy, cz, a64)
+#define FE_CALLP(l) fe_pair_fix64<l, NP>(buf + t * S64, cx, cy, cz, a64)
             FE_MX_SWITCH(FE_CALLP)
 #undef FE_CALLP
           }
+          __syncthreads();                            // buf free for the next batch
         }
       }
     }
-  } else {
-    fe_flag(FE_ST_OVERFLOW);
   }
   if (a.n64 && lane == 0) atomicAdd(a.n64, (unsigned long long)n64);
 #pragma unroll

@@ -67,7 +67,7 @@ int sm_count() {
 #define FE_NP64 2
 #endif
 #ifndef FE_MINB64
-#define FE_MINB64 3
+#define FE_MINB64 4
 #endif
 #ifndef FE_MINB32
 #define FE_MINB32 3
