@@ -465,6 +465,33 @@ def cpu_baseline(wfn, basis, P, pts, counts=None, budget_s=20.0, per_class=None)
             "build_s": t_build, "eval_s_estimated": t_eval, "n_pairs": int(tab.n_pairs)}
 
 
+def reference_cuda(wfn, basis, P, pts, repeats=5):
+    """The reference's --backend cuda pipeline (fastesp/cli.py:143-168): its C++
+    builder, then its CUDA evaluator (both compiled from the reference sources
+    into oracle/_ref), timed as the reference times them: builder wall time,
+    evaluator as the minimum of its own per-run timings."""
+    import re
+    from fastesp_b200 import basis_payload, write_basis_payload
+    bp, eg = ROOT / "oracle" / "_ref" / "build_pairs", ROOT / "oracle" / "_ref" / "esp_gpu"
+    if not (bp.exists() and eg.exists()):
+        return {"unavailable": "oracle/_ref/build_pairs or esp_gpu not built"}
+    env = dict(os.environ, OMP_NUM_THREADS=str(len(os.sched_getaffinity(0))))
+    with tempfile.TemporaryDirectory() as td:
+        bb, pb, out = Path(td) / "basis.bin", Path(td) / "pairs.bin", Path(td) / "esp.txt"
+        write_basis_payload(bb, basis_payload(wfn, basis, P, pts))
+        t0 = time.perf_counter()
+        subprocess.run([str(bp), str(bb), str(pb), "1e-12"], check=True, env=env, capture_output=True)
+        t_build = time.perf_counter() - t0
+        r = subprocess.run([str(eg), str(pb), str(out), "--repeats", str(repeats)], check=True,
+                           capture_output=True, text=True)
+        ms = min(float(m) for m in re.findall(r"run \d+: ([0-9.]+) ms", r.stdout))
+    return {"build_s": t_build, "solve_ms": ms, "points": int(len(pts)),
+            "solve_points_per_s": len(pts) / (ms * 1e-3),
+            "e2e_points_per_s": len(pts) / (t_build + ms * 1e-3),
+            "what": "reference build_pairs (OpenMP, all cores) + reference esp_gpu (FP64 CUDA, "
+                    "compiled for sm_100a), min of its own per-run host timings"}
+
+
 def run_reference(args):
     rank, world, _ = rank_info()
     if rank != 0:
@@ -490,6 +517,12 @@ def run_reference(args):
             "cpu_baseline": base,
             "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    try:
+        import torch
+        if torch.cuda.is_available():
+            line["reference_cuda"] = reference_cuda(wfn, basis, P, pts)
+    except Exception as e:                      # reported, never fatal for the CPU arm
+        line["reference_cuda"] = {"unavailable": f"{type(e).__name__}: {e}"[:200]}
     print(json.dumps(line))
 
 
