@@ -43,9 +43,7 @@ PUBLISHED = {"e2e_points_per_s": 30000 / 2.4564, "hardware": "RTX 5090",
              "source": "reference README.md:48 (table build + GPU solve, 30000 points)"}
 
 
-def rank_info():
-    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
-            int(os.environ.get("LOCAL_RANK", 0)))
+from fastesp_b200.shard import rank_info, rank_points  # noqa: E402
 
 
 # ---------------------------------------------------------------------------
@@ -142,7 +140,7 @@ def run_ours(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     wfn, basis, P, _ = synth.load_workload("frag54", 10, seed=0)
-    pts = synth.vdw_surface_points(wfn.symbols, wfn.coords, args.points, seed=1 + rank)
+    pts = rank_points(wfn.symbols, wfn.coords, args.points, rank)    # weak scaling
     dev = torch.device("cuda", local)
     P_d = torch.as_tensor(P, device=dev)
     pts_d = torch.as_tensor(pts, device=dev)
