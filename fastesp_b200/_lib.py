@@ -96,6 +96,12 @@ _SIGS = {
                                  C.POINTER(C.c_int)]),
     "fe_batch_upload": (C.c_int, [_P, _P, C.c_size_t, _P]),
     "fe_batch_run": (C.c_int, [_P, _P, _P, C.c_size_t, _P]),
+    "fe_points_ws_bytes": (C.c_size_t, [C.c_longlong]),
+    "fe_surface_points": (C.c_int, [_P, _P, C.c_int, _P, C.c_longlong, C.c_double, _P,
+                                    C.c_longlong, _P, _P, C.c_size_t, _P]),
+    "fe_grid_points": (C.c_int, [_P, C.c_int, C.c_double, _P, C.c_longlong, _P,
+                                 C.c_longlong, C.c_longlong, C.c_longlong,
+                                 _P, C.c_longlong, _P, _P, C.c_size_t, _P]),
 }
 
 _lock = threading.Lock()

@@ -180,12 +180,19 @@ class Basis:
             os_ += ns
         return t
 
-    def density_matrix_cartesian(self, min_occ: float = 1e-10) -> np.ndarray:
-        """P_cart = T (C_occ n C_occ^T) T^T (fastesp/basis.py:264-270)."""
+    def density_matrix_cartesian(self, min_occ: float = 1e-10, device=None):
+        """P_cart = T (C_occ n C_occ^T) T^T (fastesp/basis.py:264-270).
+
+        With ``device`` (a CUDA device) the two products run there as FP64
+        GEMMs and the result is a CUDA tensor; otherwise NumPy."""
         w = self.wfn
         occ = w.mo_occ > min_occ
         c = w.mo_coeff[:, occ] * np.sqrt(w.mo_occ[occ])[None, :]
         t = self.block_transform()
+        if device is not None:
+            import torch
+            tc = torch.as_tensor(t, device=device) @ torch.as_tensor(c, device=device)
+            return tc @ tc.T
         tc = t @ c
         return tc @ tc.T
 

@@ -23,6 +23,7 @@
 #include "build.cuh"
 #include "adjoint.cuh"
 #include "batch.cuh"
+#include "points.cuh"
 #include "../../include/fastesp_b200.h"
 
 static_assert(FE_NCLASS <= FE_NCLASS_MAX, "class count");
@@ -1200,6 +1201,97 @@ int fe_batch_run(const fe_batch* b, const void* d_desc, void* d_ws, size_t ws_by
     fe_batch_reduce_kernel<<<unsigned((b->total_pts + 255) / 256), 256, 0, st>>>(desc, partial);
   FE_CUDA(cudaGetLastError());
   return FE_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Evaluation points
+// ---------------------------------------------------------------------------
+namespace {
+
+struct PointWs {
+  size_t cand, keep, pos, bsum, bytes;
+  long long nb;
+};
+
+PointWs point_ws(long long ncand) {
+  PointWs w{};
+  size_t o = 0;
+  auto put = [&](size_t bytes) { const size_t at = o; o = align256(o + bytes); return at; };
+  w.cand = put(size_t(ncand) * 3 * sizeof(double));
+  w.keep = put(size_t(ncand + 1) * sizeof(int));
+  w.pos = put(size_t(ncand + 1) * sizeof(int));
+  w.nb = (ncand + FE_SCAN_BLOCK - 1) / FE_SCAN_BLOCK;
+  w.bsum = put(size_t(w.nb + 1) * sizeof(int));
+  w.bytes = std::max<size_t>(o, 256);
+  return w;
+}
+
+int point_run(const char* who, FePointArgs a, double* d_out, long long cap, int* d_count,
+              void* d_ws, size_t ws_bytes, cudaStream_t st) {
+  if (a.ncand < 0 || a.ncand >= (1LL << 31)) return fail(FE_ERR_SIZE, "%s: bad candidate count", who);
+  if (!d_out || !d_count) return fail(FE_ERR_ARG, "%s: null output", who);
+  const PointWs w = point_ws(a.ncand);
+  if (!d_ws || ws_bytes < w.bytes) return fail(FE_ERR_SIZE, "%s: workspace %zu < %zu bytes", who, ws_bytes, w.bytes);
+  if (a.ncand == 0) {
+    FE_CUDA(cudaMemsetAsync(d_count, 0, sizeof(int), st));
+    return FE_OK;
+  }
+  unsigned char* wb = static_cast<unsigned char*>(d_ws);
+  a.cand = reinterpret_cast<double*>(wb + w.cand);
+  a.keep = reinterpret_cast<int*>(wb + w.keep);
+  int* pos = reinterpret_cast<int*>(wb + w.pos);
+  int* bsum = reinterpret_cast<int*>(wb + w.bsum);
+  const unsigned nblk = unsigned((a.ncand + 255) / 256);
+  fe_point_candidates_kernel<<<nblk, 256, 0, st>>>(a);
+  fe_scan_sums_kernel<<<unsigned(w.nb), FE_SCAN_BLOCK, 0, st>>>(a.keep, a.ncand, bsum);
+  fe_scan_top_kernel<<<1, FE_SCAN_BLOCK, 0, st>>>(bsum, int(w.nb));
+  fe_scan_apply_kernel<<<unsigned(w.nb), FE_SCAN_BLOCK, 0, st>>>(a.keep, a.ncand, bsum, pos);
+  fe_point_compact_kernel<<<nblk, 256, 0, st>>>(a.cand, a.keep, pos, a.ncand, d_out, cap, d_count);
+  FE_CUDA(cudaGetLastError());
+  return FE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t fe_points_ws_bytes(long long ncand) { return ncand < 0 ? 0 : point_ws(ncand).bytes; }
+
+int fe_surface_points(const double* d_xyz, const double* d_rad, int natom, const long long* d_off,
+                      long long ncand, double slack, double* d_out, long long cap, int* d_count,
+                      void* d_ws, size_t ws_bytes, cudaStream_t st) {
+  if (natom <= 0 || !d_xyz || !d_rad || !d_off) return fail(FE_ERR_ARG, "fe_surface_points: bad atoms");
+  FePointArgs a{};
+  a.xyz = d_xyz;
+  a.rad = d_rad;
+  a.natom = natom;
+  a.slack = slack;
+  a.off = d_off;
+  a.grid = 0;
+  a.ncand = ncand;
+  return point_run("fe_surface_points", a, d_out, cap, d_count, d_ws, ws_bytes, st);
+}
+
+int fe_grid_points(const double* d_xyz, int natom, double exclude, const long long* d_index,
+                   long long ncand, const double* d_axes, long long nx, long long ny, long long nz,
+                   double* d_out, long long cap, int* d_count, void* d_ws, size_t ws_bytes,
+                   cudaStream_t st) {
+  if (natom < 0 || (natom > 0 && !d_xyz) || !d_index || !d_axes || nx <= 0 || ny <= 0 || nz <= 0)
+    return fail(FE_ERR_ARG, "fe_grid_points: bad argument");
+  FePointArgs a{};
+  a.xyz = d_xyz;
+  a.natom = natom;
+  a.excl = exclude;
+  a.index = d_index;
+  a.axes = d_axes;
+  a.nx = nx;
+  a.ny = ny;
+  a.nz = nz;
+  a.grid = 1;
+  a.ncand = ncand;
+  return point_run("fe_grid_points", a, d_out, cap, d_count, d_ws, ws_bytes, st);
 }
 
 }  // extern "C"

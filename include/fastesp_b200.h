@@ -252,6 +252,25 @@ int fe_batch_upload(const fe_batch* batch, void* d_desc, size_t desc_bytes, cuda
 int fe_batch_run(const fe_batch* batch, const void* d_desc, void* d_ws, size_t ws_bytes,
                  cudaStream_t stream);
 
+/* Evaluation points on the GPU (the reference does this in NumPy:
+ * benchmarks/make_points.py:22-58, examples/vdw_surface_esp.py:38-52).
+ * fe_surface_points: atom a contributes d_off[a+1]-d_off[a] Fibonacci points
+ * on its sphere (centre d_xyz[a], radius d_rad[a]); the candidates lying on the
+ * exposed union of the spheres (distance >= d_rad[b] - slack to every atom b,
+ * slack 1e-9 in the reference) are written, in candidate order, to d_out
+ * (capacity cap points) and their number to *d_count.  fe_grid_points: the
+ * candidates are flat indices d_index (x-major) into the nx*ny*nz grid whose
+ * axis coordinates are d_axes = [x(nx), y(ny), z(nz)]; kept when farther than
+ * ``exclude`` from every nucleus.  Workspace: fe_points_ws_bytes(ncand). */
+size_t fe_points_ws_bytes(long long ncand);
+int fe_surface_points(const double* d_xyz, const double* d_rad, int natom, const long long* d_off,
+                      long long ncand, double slack, double* d_out, long long cap, int* d_count,
+                      void* d_ws, size_t ws_bytes, cudaStream_t stream);
+int fe_grid_points(const double* d_xyz, int natom, double exclude, const long long* d_index,
+                   long long ncand, const double* d_axes, long long nx, long long ny, long long nz,
+                   double* d_out, long long cap, int* d_count, void* d_ws, size_t ws_bytes,
+                   cudaStream_t stream);
+
 /* FMA throughput probe (no counterpart in the reference): ``blocks`` blocks of
  * 256 threads each run ``iters`` iterations of 8 independent FMA chains in FP64
  * (fp64 != 0) or FP32, writing one value per block to d_out.  Timed by the
