@@ -116,6 +116,8 @@ FE_DEV void fe_boys_f32(const float T, const float rt, const float* __restrict__
 // the tabulated and the asymptotic branch only.  Each lane gets what
 // fe_boys_f32 gives it (the same operations lane by lane); when the lanes fall
 // in different branches both are computed and each lane keeps its own.
+// ``grid`` holds the per-order scaled rows fe_boys_grid32s (F_(M+k)/k!), so the
+// Taylor polynomial is evaluated in d directly.
 template <int M>
 FE_DEV void fe_boys_f32x2(const float2 T, const float2 rt, const float* __restrict__ grid,
                           float2 (&F)[M + 1]) {
@@ -135,12 +137,11 @@ FE_DEV void fe_boys_f32x2(const float2 T, const float2 rt, const float* __restri
     const int ix = min(max(__float2int_rn(ti.x), 0), FE_BOYS32_NROW - 1);
     const int iy = min(max(__float2int_rn(ti.y), 0), FE_BOYS32_NROW - 1);
     const float2 d = make_float2(float(ix), float(iy)) * fe_f2(FE_BOYS32_GRID_H) - T;   // exact
-    const float* rx = grid + ix * FE_BOYS32_NTAB + M;
-    const float* ry = grid + iy * FE_BOYS32_NTAB + M;
+    const float* rx = grid + (M * FE_BOYS32_NROW + ix) * FE_BOYS32_TAYLOR_K;
+    const float* ry = grid + (M * FE_BOYS32_NROW + iy) * FE_BOYS32_TAYLOR_K;
     float2 f = make_float2(rx[FE_BOYS32_TAYLOR_K - 1], ry[FE_BOYS32_TAYLOR_K - 1]);
 #pragma unroll
-    for (int k = FE_BOYS32_TAYLOR_K - 2; k >= 0; --k)
-      f = fe_fma(f, d * fe_f2(1.0f / float(k + 1)), make_float2(rx[k], ry[k]));
+    for (int k = FE_BOYS32_TAYLOR_K - 2; k >= 0; --k) f = fe_fma(f, d, make_float2(rx[k], ry[k]));
     G[M] = f;
     const float2 e = make_float2(__expf(-T.x), __expf(-T.y));
     const float2 t2 = T + T;

@@ -209,7 +209,10 @@ FE_DEV bool fe_route2(const float* __restrict__ rec, const float2 (&cxh)[NQ],
                       const float2 (&cyl)[NQ], const float2 (&czl)[NQ], float2 (&x)[NQ],
                       float2 (&y)[NQ], float2 (&z)[NQ], float2 (&r2)[NQ], float2 (&ir)[NQ],
                       float tau) {
-  const float kb = rec[10];
+  // K*bound/|R| >= tau  <=>  |R|^2 <= (K*bound/tau)^2 (also for K*bound = +inf);
+  // ``tau`` here is 1/tau
+  const float reach = __fmul_rn(rec[10], tau);
+  const float reach2 = __fmul_rn(reach, reach);
   const float2 pxh = fe_f2(rec[2]), pyh = fe_f2(rec[3]), pzh = fe_f2(rec[4]);
   const float2 pxl = fe_f2(rec[5]), pyl = fe_f2(rec[6]), pzl = fe_f2(rec[7]);
   bool need = false;
@@ -220,7 +223,7 @@ FE_DEV bool fe_route2(const float* __restrict__ rec, const float2 (&cxh)[NQ],
     z[q] = (czh[q] - pzh) + (czl[q] - pzl);
     r2[q] = fe_fma(x[q], x[q], fe_fma(y[q], y[q], z[q] * z[q]));
     ir[q] = make_float2(rsqrtf(r2[q].x), rsqrtf(r2[q].y));
-    need |= !(__fmul_rn(kb, ir[q].x) < tau) || !(__fmul_rn(kb, ir[q].y) < tau);
+    need |= (r2[q].x <= reach2) || (r2[q].y <= reach2);
   }
   return __any_sync(0xffffffffu, need);
 }
@@ -230,7 +233,7 @@ FE_DEV void fe_tile_f32x2(const float* __restrict__ rec, int first, int n, int h
                           const float2 (&cxh)[NQ], const float2 (&cyh)[NQ],
                           const float2 (&czh)[NQ], const float2 (&cxl)[NQ],
                           const float2 (&cyl)[NQ], const float2 (&czl)[NQ], float2 (&ahi)[NQ],
-                          float2 (&alo)[NQ], const float* __restrict__ grid, float tau,
+                          float2 (&alo)[NQ], const float* __restrict__ grid, float inv_tau,
                           unsigned* __restrict__ mw, unsigned& bits) {
   constexpr int S32 = fe_class_rec32[L];
   const bool lane0 = (threadIdx.x & 31) == 0;
@@ -238,7 +241,7 @@ FE_DEV void fe_tile_f32x2(const float* __restrict__ rec, int first, int n, int h
   for (int i = 0; i < n; ++i, rec += S32) {
     const int gi = first + i;
     float2 x[NQ], y[NQ], z[NQ], r2[NQ], ir[NQ];
-    const bool routed = fe_route2<NQ>(rec, cxh, cyh, czh, cxl, cyl, czl, x, y, z, r2, ir, tau);
+    const bool routed = fe_route2<NQ>(rec, cxh, cyh, czh, cxl, cyl, czl, x, y, z, r2, ir, inv_tau);
     bits |= unsigned(routed) << (gi & 31);
     if ((gi & 31) == 31 || gi + 1 == hi) {
       if (lane0 && mw) mw[gi >> 5] = bits;
@@ -302,10 +305,13 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
   extern __shared__ __align__(128) unsigned char fe_smem[];
   __shared__ uint64_t full_bar[FE_NSTAGE];
   __shared__ FeBlockWork w;
-  __shared__ float grid[FE_BOYS32_NROW * FE_BOYS32_NTAB];
+  // packed classes: the per-order scaled rows; g-shell classes: the plain rows
+  constexpr int GRIDN = PACKED ? (FE_BOYS32S_MMAX + 1) * FE_BOYS32_NROW * FE_BOYS32_TAYLOR_K
+                               : FE_BOYS32_NROW * FE_BOYS32_NTAB;
+  __shared__ float grid[GRIDN];
   const FeTableHdr* hdr = reinterpret_cast<const FeTableHdr*>(a.table);
   const int tid = threadIdx.x;
-  for (int k = tid; k < FE_BOYS32_NROW * FE_BOYS32_NTAB; k += NT) grid[k] = fe_boys_grid32[k];
+  for (int k = tid; k < GRIDN; k += NT) grid[k] = PACKED ? fe_boys_grid32s[k] : fe_boys_grid32[k];
   float cxh[NP], cyh[NP], czh[NP], cxl[NP], cyl[NP], czl[NP], ahi[NP], alo[NP];
   const int p0 = int(blockIdx.x) * (NT * NP) + tid;
   fe_load_points_split<NP>(a.pts, a.npts, p0, NT, cxh, cyh, czh, cxl, cyl, czl);
@@ -335,6 +341,7 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
     fe_flag(FE_ST_OVERFLOW);
   }
   unsigned bits = 0u;
+  const float inv_tau = 1.0f / a.tau;
   for (int i = 0; i < total; ++i) {
     if (!pipe.wait(i)) {
       pipe.abort(i);
@@ -346,7 +353,7 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
     unsigned* mw = mrow ? mrow + w.woff[L] : nullptr;
     if constexpr (PACKED) {
 #define FE_CALL32(l) fe_tile_f32x2<l, NQ>(rec, first, n, w.hi[L], cxh2, cyh2, czh2, cxl2, cyl2, \
-                                          czl2, ahi2, alo2, grid, a.tau, mw, bits)
+                                          czl2, ahi2, alo2, grid, inv_tau, mw, bits)
       FE_MX_SWITCH(FE_CALL32)
 #undef FE_CALL32
     } else {

@@ -369,6 +369,15 @@ def boys_grid32():
             for i in range(nrow)]
 
 
+def boys_grid32_scaled(M):
+    """Rows F_(M+k)(i h)/k!, k < TAYLOR_K32, of the FP32 grid (30 digits)."""
+    import mpmath as mp
+    mp.mp.dps = 30
+    nrow = int(round(GRID_TMAX32 / GRID_H32)) + 2
+    return [[float(boys_mp(M + k, mp.mpf(i) * mp.mpf(GRID_H32)) / mp.factorial(k))
+             for k in range(TAYLOR_K32)] for i in range(nrow)]
+
+
 def asym_thresholds(rel=1e-16):
     """Smallest T (on a 0.25 grid) from which the asymptotic Boys vector
     F_m = (2m-1)!!/2^(m+1) sqrt(pi/T^(2m+1)) is within ``rel`` of F_m for all
@@ -441,6 +450,18 @@ def main() -> int:
     out.append("__device__ const float fe_boys_grid32[FE_BOYS32_NROW * FE_BOYS32_NTAB] = {")
     for r in rows32:
         out.append("  " + ", ".join(repr(float(v)) + "f" if v > 1e-37 else "0.0f" for v in r) + ",")
+    out.append("};")
+    out.append("")
+    # per-order scaled FP32 rows for the packed evaluator: F_(M+k)(i h) / k!
+    ms = 6
+    out.append(f"#define FE_BOYS32S_MMAX {ms}")
+    out.append("// F_(M+k)(i h)/k!, M = 0..FE_BOYS32S_MMAX, k < FE_BOYS32_TAYLOR_K: row (M, i) at")
+    out.append("// (M * FE_BOYS32_NROW + i) * FE_BOYS32_TAYLOR_K (Taylor polynomial in d directly)")
+    out.append("__device__ const float fe_boys_grid32s[(FE_BOYS32S_MMAX + 1) * FE_BOYS32_NROW"
+               " * FE_BOYS32_TAYLOR_K] = {")
+    for M in range(ms + 1):
+        for i, r in enumerate(boys_grid32_scaled(M)):
+            out.append("  " + ", ".join(repr(float(v)) + "f" if abs(v) > 1e-37 else "0.0f" for v in r) + ",")
     out.append("};")
     out.append("")
     # Boys grid
