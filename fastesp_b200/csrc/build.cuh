@@ -331,40 +331,61 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
   const double bound = pow(tp, -1.5) * bsum;
   const double reff = 1.6 * sqrt((L + 2.0) / p);
 
-  // Nearest point, exactly as the reference computes it (IEEE arithmetic, no
-  // contraction: the minimum of ((dx^2 + dy^2) + dz^2) over the points), found
-  // by a search over 1024-point superblocks and 32-point blocks that skips a
-  // box whose distance lower bound exceeds the best distance so far -- the
-  // minimum is the brute-force one -- and stops early once the pair is kept
-  // whatever the remaining points are (the bound test below, with a 1e-9
-  // relative margin far above rounding).
+  // Point screen with the reference's decision (keep unless
+  // K bound / max(d, 0.05) < tol, d = dmin or dmin - reff, dmin the exact
+  // IEEE minimum of ((dx^2 + dy^2) + dz^2) over the points), decided without
+  // the full minimum where the answer is certain: with r* = K bound / tol,
+  //  * r* < 0.05 (1 - 1e-9): dropped, whatever dmin is;
+  //  * only points within rcut = (r* (1 + 1e-9) [+ reff]) can matter: boxes of
+  //    32 points (and superboxes of 1024) whose distance lower bound exceeds
+  //    rcut, or the best distance so far, are skipped;
+  //  * a point that makes the pair kept with a 1e-9 relative margin ends the
+  //    search (kept); no point within rcut means dropped;
+  //  * otherwise the minimum over the points within rcut is the exact dmin and
+  //    the reference's formula decides.
+  // The 1e-9 margins are far above the rounding of the tests themselves.
   const double KB = __dmul_rn(K, bound);
   double d2min = 1e300;
-  bool sure = false;
+  bool sure = false, none = false;
   auto sure_keep = [&](double d2) {
     double d = __dsqrt_rn(d2);
     if (a.rule == 1) d = d - reff;
     return KB >= a.tol * (1.0 + 1e-9) * fmax(d, 0.05);
   };
-  for (int sb = 0; sb < a.nsbox && !sure; ++sb) {
-    if (fe_box_lb2(a.sbox + 6 * sb, P) * (1.0 - 1e-12) > d2min) continue;
-    const int b1 = min(32 * sb + 32, a.nbox);
-    for (int b = 32 * sb; b < b1; ++b) {
-      if (fe_box_lb2(a.box + 6 * b, P) * (1.0 - 1e-12) > d2min) continue;
-      const int q1 = min(32 * b + 32, a.npts);
-      for (int q = 32 * b; q < q1; ++q) {
-        const double dx = __dsub_rn(a.pts[3 * q], P[0]);
-        const double dy = __dsub_rn(a.pts[3 * q + 1], P[1]);
-        const double dz = __dsub_rn(a.pts[3 * q + 2], P[2]);
-        const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-        d2min = fmin(d2min, d2);
+  if (a.npts > 0 && a.tol > 0.0) {
+    const double rstar = KB / a.tol;
+    if (rstar < 0.05 * (1.0 - 1e-9)) {
+      none = true;
+    } else {
+      const double rcut = (rstar * (1.0 + 1e-9) + (a.rule == 1 ? reff : 0.0)) * (1.0 + 1e-12);
+      const double rcut2 = rcut * rcut;
+      for (int sb = 0; sb < a.nsbox && !sure; ++sb) {
+        const double ls = fe_box_lb2(a.sbox + 6 * sb, P) * (1.0 - 1e-12);
+        if (ls > rcut2 || ls > d2min) continue;
+        const int b1 = min(32 * sb + 32, a.nbox);
+        for (int b = 32 * sb; b < b1; ++b) {
+          const double lb = fe_box_lb2(a.box + 6 * b, P) * (1.0 - 1e-12);
+          if (lb > rcut2 || lb > d2min) continue;
+          const int q1 = min(32 * b + 32, a.npts);
+          for (int q = 32 * b; q < q1; ++q) {
+            const double dx = __dsub_rn(a.pts[3 * q], P[0]);
+            const double dy = __dsub_rn(a.pts[3 * q + 1], P[1]);
+            const double dz = __dsub_rn(a.pts[3 * q + 2], P[2]);
+            const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+            if (d2 <= rcut2) d2min = fmin(d2min, d2);
+          }
+          if (d2min < 1e300 && sure_keep(d2min)) {
+            sure = true;
+            break;
+          }
+        }
       }
-      if (sure_keep(d2min)) {
-        sure = true;
-        break;
-      }
+      none = !sure && !(d2min < 1e300);
     }
+  } else {
+    sure = true;                       // no points, or tol 0: every pair is kept
   }
+  if (none) return;
   double dd = __dsqrt_rn(d2min);
   if (a.rule == 1) dd = dd - reff;
   dd = fmax(dd, 0.05);
