@@ -6,14 +6,17 @@
 //  * routing: for every pair and every point the bound K*bound/|R| (the
 //    reference's screening bound, fastesp/esp.py:251-254, evaluated at the
 //    point) bounds sum_k |G_k R^a F_m|; when it reaches ``tau`` for any point
-//    of a warp's point set, that (pair, warp) is evaluated in FP64 instead.
-//    fe_eval_f32_kernel takes the decision (fe_route), evaluates every
-//    (pair, warp) left in FP32 and records the others as one bit per
-//    (pair, warp) in a routing mask in the workspace; fe_eval_fix64_kernel
-//    walks the set bits and evaluates exactly those pairs in FP64, fetching
-//    only their FP64 records.  Neither kernel carries the other's code, so
-//    each keeps its registers.  1/|R| comes from the rsqrt that the FP32 Boys
-//    function needs anyway (T^-1/2 = p^-1/2 / |R|).
+//    of a warp's point set (tested as |R|^2 <= (K*bound/tau)^2), that
+//    (pair, warp) is evaluated in FP64 instead.  fe_eval_f32_kernel takes the
+//    decision, evaluates every (pair, warp) left in FP32 and records the others
+//    as one bit per (pair, warp) in a routing mask in the workspace;
+//    fe_eval_fix64_kernel evaluates exactly those in FP64 from the pairs' FP64
+//    records.  Neither kernel carries the other's code, so each keeps its
+//    registers.
+//  * the classes up to 6 run two points per packed FP32x2 lane (sm_100
+//    __ffma2_rn / __fadd2_rn / __fmul2_rn), with the coefficients stored twice
+//    in the FP32 records so that a 16-byte load gives two packed operands; the
+//    g-shell classes run scalar.
 //  * R = C - P from float hi/lo splits of both coordinates, so R carries about
 //    one float ulp of R itself rather than of |C|.
 //  * accumulation: FP32 contributions into a compensated two-sum pair per
@@ -21,13 +24,13 @@
 //    contributions into an FP64 sum; the splits, the nuclear term and the final
 //    nuclear - electron subtraction are FP64.
 //
-// Grid and pipeline of the FP32 kernel as eval_f64: points in registers (NP
-// per thread), record tiles streamed to shared memory by 1-D TMA bulk copies
-// over an mbarrier ring.  Both kernels use the same point blocks (FE_MX_NT
-// threads x FE_MX_NP points), so warp g covers the same points in both; its
-// mask row is words [g * wtotal, (g+1) * wtotal), class L from woff[L].  The
-// FP32 kernel's pair splits sit on multiples of 32 pairs, so every mask word
-// has exactly one writer and the mask needs no clearing.
+// Grid and pipeline of the FP32 kernel as eval_f64 (class-major grid rows,
+// points in registers, record tiles streamed to shared memory by 1-D TMA bulk
+// copies over an mbarrier ring).  Both kernels use the same point blocks
+// (FE_MX_NT threads x FE_MX_NP points), so warp g covers the same points in
+// both; its mask row is words [g * wtotal, (g+1) * wtotal), class L from
+// woff[L].  The FP32 kernel's pair parts sit on multiples of 32 pairs, so every
+// mask word has exactly one writer and the mask needs no clearing.
 #pragma once
 #include "eval_f64.cuh"
 
@@ -56,18 +59,6 @@ __constant__ int fe_c_tile32[FE_NCLASS] = {
   FE_STAGE_BYTES / (4 * fe_class_rec32[6]), FE_STAGE_BYTES / (4 * fe_class_rec32[7]),
   FE_STAGE_BYTES / (4 * fe_class_rec32[8])};
 
-// Pairs per stage of the FP64-part kernel: routing record + FP64 record.
-__constant__ int fe_c_tilefix[FE_NCLASS] = {
-  FE_STAGE_BYTES / (4 * fe_class_rec32[0] + 8 * fe_class_rec64[0]),
-  FE_STAGE_BYTES / (4 * fe_class_rec32[1] + 8 * fe_class_rec64[1]),
-  FE_STAGE_BYTES / (4 * fe_class_rec32[2] + 8 * fe_class_rec64[2]),
-  FE_STAGE_BYTES / (4 * fe_class_rec32[3] + 8 * fe_class_rec64[3]),
-  FE_STAGE_BYTES / (4 * fe_class_rec32[4] + 8 * fe_class_rec64[4]),
-  FE_STAGE_BYTES / (4 * fe_class_rec32[5] + 8 * fe_class_rec64[5]),
-  FE_STAGE_BYTES / (4 * fe_class_rec32[6] + 8 * fe_class_rec64[6]),
-  FE_STAGE_BYTES / (4 * fe_class_rec32[7] + 8 * fe_class_rec64[7]),
-  FE_STAGE_BYTES / (4 * fe_class_rec32[8] + 8 * fe_class_rec64[8])};
-
 FE_DEV void fe_two_sum(float& hi, float& lo, float b) {
   const float s = hi + b;
   const float bb = s - hi;
@@ -95,46 +86,6 @@ FE_DEV bool fe_route(const float* __restrict__ rec, const float (&cxh)[NP], cons
     need |= !(__fmul_rn(kb, ir[j]) < tau);
   }
   return __any_sync(0xffffffffu, need);
-}
-
-// Bounding sphere of the warp's points (from the float coordinates), equal in
-// every lane.  The radius carries a 1e-3 Bohr margin.
-template <int NP>
-FE_DEV void fe_warp_sphere(const float (&cxh)[NP], const float (&cyh)[NP], const float (&czh)[NP],
-                           float& ox, float& oy, float& oz, float& rad) {
-  float sx = 0.f, sy = 0.f, sz = 0.f;
-#pragma unroll
-  for (int j = 0; j < NP; ++j) { sx += cxh[j]; sy += cyh[j]; sz += czh[j]; }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    sx += __shfl_xor_sync(0xffffffffu, sx, o);
-    sy += __shfl_xor_sync(0xffffffffu, sy, o);
-    sz += __shfl_xor_sync(0xffffffffu, sz, o);
-  }
-  ox = sx * (1.0f / (32 * NP));
-  oy = sy * (1.0f / (32 * NP));
-  oz = sz * (1.0f / (32 * NP));
-  float r2 = 0.f;
-#pragma unroll
-  for (int j = 0; j < NP; ++j) {
-    const float dx = cxh[j] - ox, dy = cyh[j] - oy, dz = czh[j] - oz;
-    r2 = fmaxf(r2, dx * dx + dy * dy + dz * dz);
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) r2 = fmaxf(r2, __shfl_xor_sync(0xffffffffu, r2, o));
-  rad = sqrtf(r2) + 1e-3f;
-}
-
-// True when no point of the warp can be routed to FP64 for this pair: every
-// point lies farther than its routing radius K*bound/tau (with a 0.1% + 1e-3
-// Bohr margin, far above the float rounding of the per-point test, so that
-// fe_route would also have answered "FP32" for every point).
-FE_DEV bool fe_out_of_reach(const float* __restrict__ rec, float ox, float oy, float oz,
-                            float rad, float inv_tau) {
-  const float dx = rec[2] - ox, dy = rec[3] - oy, dz = rec[4] - oz;
-  const float d = sqrtf(dx * dx + dy * dy + dz * dz) - rad;
-  const float reach = rec[10] * inv_tau * 1.001f + 1e-3f;
-  return d > reach;
 }
 
 template <int NP>
