@@ -13,6 +13,8 @@ the shapes of the reference's benchmark system:
 * ``tz``      : ``natom`` atoms (default 6) of the frag54 recipe (all classes L=0..6).
 * ``adjoint20``: 20 atoms of the same recipe with an l<=2 basis (~270 functions).
 * ``batch``   : molecules of 5-60 atoms with l<=2 bases.
+* ``qz``      : a few atoms whose heavy atoms also carry a g shell (classes up
+  to L = 8, the g-shell kernel instances).
 
 Contraction coefficients are drawn uniform in [0.1, 1] and multiplied by the
 radial factor N_s(a, l) that MOLDEN coefficients carry (the convention
@@ -46,6 +48,7 @@ _TZ_HEAVY = [(0, 4, (1.0, 3.7)), (0, 1, (-0.1, 0.5)), (0, 1, (-0.8, -0.3)),
              (3, 1, (-0.4, 0.1))]
 _TZ_H = [(0, 3, (-0.5, 1.6)), (0, 1, (-1.0, -0.5)), (0, 1, (-1.7, -1.2)),
          (1, 1, (-0.5, 0.1))]
+_QZ_HEAVY = _TZ_HEAVY + [(4, 1, (-0.3, 0.2))]     # adds a g shell (classes up to L = 8)
 _DZ_HEAVY = [(0, 4, (0.5, 3.5)), (0, 1, (-0.3, 0.3)), (0, 1, (-1.0, -0.5)),
              (1, 3, (-0.3, 1.5)), (1, 1, (-1.0, -0.5)),
              (2, 1, (-0.4, 0.1))]
@@ -174,6 +177,14 @@ def make_system(name: str, seed: int = 0, natom: int | None = None) -> System:
         symbols = [str(x) for x in rng.choice(comp, size=n, replace=n > len(comp))]
         coords = _chain_geometry(rng, symbols, bond=(1.0, 1.6))
         shells = _draw_shells(rng, symbols, _TZ_HEAVY, _TZ_H)
+    elif name == "qz":
+        n = natom if natom is not None else 4
+        comp = np.array(["C"] * 30 + ["N"] * 8 + ["O"] * 8 + ["H"] * 8)
+        symbols = [str(x) for x in rng.choice(comp, size=n, replace=n > len(comp))]
+        if all(s == "H" for s in symbols):
+            symbols[0] = "C"
+        coords = _chain_geometry(rng, symbols, bond=(1.0, 1.6))
+        shells = _draw_shells(rng, symbols, _QZ_HEAVY, _TZ_H)
     elif name in ("adjoint20", "batch"):
         n = natom if natom is not None else 20
         comp = np.array(["C"] * 30 + ["N"] * 8 + ["O"] * 8 + ["H"] * 8)
