@@ -150,3 +150,33 @@ def test_synthetic_workload_shapes():
     d = np.linalg.norm(pts[:, None, :] - s.coords[None], axis=2)
     assert (d >= rad[None, :] - 1e-9).all()
     assert np.isclose(d / rad[None, :], 1.0, atol=1e-9).any(axis=1).all()
+
+
+def test_generated_adjoint_chunks_partition_terms():
+    """The adjoint moment chunks cover every term once, in order, never split a
+    monomial's terms, and keep at most MOM_CHUNK accumulators."""
+    import importlib.util
+    from pathlib import Path
+    from fastesp_b200 import hermite as H
+    spec = importlib.util.spec_from_file_location(
+        "gen_classes", Path(__file__).resolve().parents[1] / "fastesp_b200" / "csrc" / "gen_classes.py")
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    for L in range(9):
+        keys, _ = H.class_terms(L)
+        spans = gen.mom_chunks(L)
+        assert spans[0][0] == 0 and spans[-1][1] == len(keys)
+        for (a0, b0), (a1, b1) in zip(spans, spans[1:]):
+            assert b0 == a1
+        for a, b in spans:
+            assert 0 < b - a <= gen.MOM_CHUNK
+            if a > 0:
+                assert keys[a][:3] != keys[a - 1][:3]
+
+
+def test_record_strides_are_16_byte_multiples():
+    from fastesp_b200 import hermite as H
+    for L in range(9):
+        nt = H.n_terms(L)
+        assert H.record_stride(L) * 8 % 16 == 0 and H.record_stride(L) >= 6 + nt
+        assert H.record_stride_f32(L) * 4 % 16 == 0 and H.record_stride_f32(L) >= 12 + 2 * nt
