@@ -125,6 +125,20 @@ def peak_flops(torch, fp64=True):
     return best
 
 
+def hbm_view(traffic, ms):
+    """The memory side of the dominant kernel: its ncu DRAM bytes per launch over
+    the step time, against the measured HBM copy bandwidth (MEASURED_PEAKS.json)."""
+    peaks = ROOT / "MEASURED_PEAKS.json"
+    if traffic is None or not peaks.exists():
+        return None
+    gbs = json.loads(peaks.read_text()).get("hbm_gbs")
+    if not gbs:
+        return None
+    achieved = traffic / (ms * 1e-3) / 1e9
+    return {"achieved": achieved, "peak": gbs, "unit": "GB/s", "frac": achieved / gbs,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"}
+
+
 def algorithmic_flops(counts, npts):
     from fastesp_b200 import hermite as H
     return float(sum(c * H.eval_flops(L) for L, c in enumerate(counts))) * npts
@@ -303,7 +317,8 @@ def run_ours(args):
                      "peak_source": "measured FMA throughput (fe_peak_run) on this GPU, this run",
                      "flops_per_step": flops,
                      "fp64_path": {"achieved": flops / (ms_fp64 * 1e-3) / 1e12,
-                                   "peak": peak64 / 1e12, "frac": flops / (ms_fp64 * 1e-3) / peak64}},
+                                   "peak": peak64 / 1e12, "frac": flops / (ms_fp64 * 1e-3) / peak64},
+                     "hbm_view": hbm_view(traffic, ms_per_step)},
         "gpu_launches": args.steps * launches,
         "parity_frag54_300_max_abs": parity,
         "device_status": status,
