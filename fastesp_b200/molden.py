@@ -74,11 +74,55 @@ def _float(tok: str) -> float:
     return float(tok.replace("D", "E").replace("d", "e"))
 
 
+def _coefficient_block(block: list):
+    """(indices, values) of one MO's "index value" lines.  The common layout
+    (two numbers on every non-empty line) is converted in one NumPy call; any
+    other layout line by line, taking the first and the last field of a row as
+    the reference does."""
+    rows = len(block) - block.count("")
+    text = " ".join(block).replace("D", "E").replace("d", "e")
+    try:
+        arr = np.array(text.split(), dtype=np.float64)
+    except ValueError:
+        arr = None
+    if arr is not None and arr.size == 2 * rows:
+        pairs = arr.reshape(-1, 2)
+        return pairs[:, 0].astype(np.int64), pairs[:, 1].copy()
+    idx, val = [], []
+    for ln in block:
+        f = ln.split()
+        if len(f) >= 2:
+            idx.append(int(f[0]))
+            val.append(_float(f[-1]))
+    return np.asarray(idx, dtype=np.int64), np.asarray(val, dtype=np.float64)
+
+
+_HEADER_LINE = re.compile(r"^[ \t]*\[.*$", re.M)
+_SYM_LINE = re.compile(r"^[ \t]*Sym=", re.M)
+
+
+def _section_text(text: str) -> dict:
+    """Map section name -> its body text: from the end of its header line to the
+    next line that starts with ``[`` (first occurrence of a name wins)."""
+    heads = list(_HEADER_LINE.finditer(text))
+    out = {}
+    for k, m in enumerate(heads):
+        h = _SECTION.match(m.group(0).strip())
+        if not h or h.group(1).strip() in out:
+            continue
+        end = heads[k + 1].start() if k + 1 < len(heads) else len(text)
+        out[h.group(1).strip()] = text[m.end():end]
+    return out
+
+
 def _sections(lines: list) -> dict:
     """Map section name -> (header line index, trailing text); first one wins."""
     out = {}
     for i, raw in enumerate(lines):
-        m = _SECTION.match(raw.strip())
+        t = raw.strip()
+        if not t.startswith("["):           # cheap test before the regex
+            continue
+        m = _SECTION.match(t)
         if m and m.group(1).strip() not in out:
             out[m.group(1).strip()] = (i, m.group(2).strip())
     return out
@@ -94,15 +138,19 @@ def _body(lines: list, start: int) -> list:
 
 
 def read_molden(path) -> Wavefunction:
-    """Parse a MOLDEN file into a :class:`Wavefunction` (atomic units)."""
-    lines = Path(path).read_text(errors="ignore").splitlines()
-    sec = _sections(lines)
+    """Parse a MOLDEN file into a :class:`Wavefunction` (atomic units).
+
+    Works on the file text: section headers are found with one multiline
+    search, each section is sliced out by offset, and every MO's coefficient
+    rows are converted in one NumPy call (the bulk of a large file)."""
+    text = Path(path).read_text(errors="ignore")
+    sec = _section_text(text)
     for need in ("Atoms", "GTO", "MO"):
         if need not in sec:
             raise ValueError(f"{path}: MOLDEN section [{need}] missing")
 
     symbols, coords = [], []
-    for raw in _body(lines, sec["Atoms"][0]):
+    for raw in sec["Atoms"].splitlines():
         m = _ATOM_LINE.match(raw)
         if m:
             symbols.append(m.group(1))
@@ -110,7 +158,7 @@ def read_molden(path) -> Wavefunction:
     coords_arr = np.asarray(coords, dtype=np.float64).reshape(-1, 3)
 
     shells = []
-    gto = _body(lines, sec["GTO"][0])
+    gto = sec["GTO"].splitlines()
     atom = -1
     i = 0
     while i < len(gto):
@@ -133,33 +181,24 @@ def read_molden(path) -> Wavefunction:
     spherical = {l: f"{2 * l + 1}{'SPDFGH'[l]}" in sec for l in range(5)}
 
     energies, occs, cols = [], [], []
-    mo = _body(lines, sec["MO"][0])
-    i = 0
-    while i < len(mo):
-        if not mo[i].strip().startswith("Sym="):
-            i += 1
-            continue
-        i += 1
+    mo = sec["MO"]
+    starts = [m.start() for m in _SYM_LINE.finditer(mo)]
+    for k, a in enumerate(starts):
+        lines = mo[a:starts[k + 1] if k + 1 < len(starts) else len(mo)].splitlines()
         ene = occ = 0.0
-        while i < len(mo):
-            t = mo[i].strip()
+        j = 1                                  # lines[0] is the Sym= line
+        while j < len(lines):
+            t = lines[j].strip()
             if t.startswith("Ene="):
                 ene = _float(t.split("=", 1)[1])
             elif t.startswith("Occup="):
                 occ = _float(t.split("=", 1)[1])
             elif not (t.startswith("Spin=") or not t):
                 break
-            i += 1
-        idx, val = [], []
-        while i < len(mo) and not mo[i].strip().startswith("Sym="):
-            f = mo[i].split()
-            if len(f) >= 2:
-                idx.append(int(f[0]))
-                val.append(_float(f[-1]))
-            i += 1
+            j += 1
         energies.append(ene)
         occs.append(occ)
-        cols.append((np.asarray(idx, dtype=np.int64), np.asarray(val)))
+        cols.append(_coefficient_block(lines[j:]))
 
     if not cols:
         raise ValueError(f"{path}: no molecular orbitals in [MO]")

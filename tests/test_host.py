@@ -180,3 +180,34 @@ def test_record_strides_are_16_byte_multiples():
         nt = H.n_terms(L)
         assert H.record_stride(L) * 8 % 16 == 0 and H.record_stride(L) >= 6 + nt
         assert H.record_stride_f32(L) * 4 % 16 == 0 and H.record_stride_f32(L) >= 12 + 2 * nt
+
+
+def test_molden_reader_fast_and_fallback_paths_agree(tmp_path):
+    """Fortran D exponents, an extra field on a row and whitespace-only lines
+    (the line-by-line path) give the same wavefunction as the plain file."""
+    import numpy as np
+    from pathlib import Path
+    from fastesp_b200 import read_molden
+    src = Path(__file__).resolve().parent / "golden" / "small.molden"
+    w0 = read_molden(src)
+    lines = src.read_text().splitlines()
+    out, in_mo = [], False
+    for ln in lines:
+        if ln.strip().startswith("[MO]"):
+            in_mo = True
+        f = ln.split()
+        if in_mo and len(f) == 2 and f[0].isdigit():
+            ln = f"{f[0]} {float(f[1]):.12E}".replace("E", "D")
+        out.append(ln)
+    # one row with three fields (first and last are used) and a blank-with-spaces line
+    for k, ln in enumerate(out):
+        f = ln.split()
+        if len(f) == 2 and "D" in f[1]:
+            out[k] = f"{f[0]} x {f[1]}"
+            out.insert(k + 1, "    ")
+            break
+    p = tmp_path / "variant.molden"
+    p.write_text("\n".join(out) + "\n")
+    w1 = read_molden(p)
+    np.testing.assert_array_equal(w1.mo_occ, w0.mo_occ)
+    np.testing.assert_allclose(w1.mo_coeff, w0.mo_coeff, rtol=1e-12, atol=0)
