@@ -115,28 +115,6 @@ def _section_text(text: str) -> dict:
     return out
 
 
-def _sections(lines: list) -> dict:
-    """Map section name -> (header line index, trailing text); first one wins."""
-    out = {}
-    for i, raw in enumerate(lines):
-        t = raw.strip()
-        if not t.startswith("["):           # cheap test before the regex
-            continue
-        m = _SECTION.match(t)
-        if m and m.group(1).strip() not in out:
-            out[m.group(1).strip()] = (i, m.group(2).strip())
-    return out
-
-
-def _body(lines: list, start: int) -> list:
-    out = []
-    for raw in lines[start + 1:]:
-        if raw.lstrip().startswith("["):
-            break
-        out.append(raw)
-    return out
-
-
 def read_molden(path) -> Wavefunction:
     """Parse a MOLDEN file into a :class:`Wavefunction` (atomic units).
 
