@@ -1,16 +1,18 @@
 // Batched FP64 evaluation: many molecules (each its own pair table and points)
 // in one persistent launch over a flattened work queue.
 //
-// A work item is (molecule, point block, pair split): the block evaluates the
-// molecule's points [pb * PPB, (pb + 1) * PPB) against split ``split`` of
-// ``nsplit`` of every class of its table and writes one row of partial sums.
-// Items are ordered by estimated cost, largest first, and taken from a global
-// counter by the resident blocks (greedy longest-first scheduling), so uneven
-// molecules and point counts fill the GPU without a tail.  Every item writes its
-// own row and fe_batch_reduce_kernel adds a molecule's rows in a fixed order,
-// so the result is bitwise independent of which block ran which item.  The
-// arithmetic per (pair, point) is that of fe_eval_f64_kernel: results equal
-// fe_esp_fp64 up to the order of the split sums.
+// A work item is (molecule, point block, class L, part): the block evaluates
+// the molecule's points [pb * PPB, (pb + 1) * PPB) against part ``part`` of
+// ``nsplit[L]`` of the class-L pairs of its table and writes one row of partial
+// sums.  The queue is class-major -- all class-0 items, then class 1, ... --
+// and within a class largest first, so the blocks that run at the same time
+// execute the same class's unrolled code (instruction-cache locality) and the
+// expensive items start early.  Resident blocks take items from a global
+// counter.  Every item writes its own row and fe_batch_reduce_kernel adds a
+// molecule's rows in a fixed order, so the result is bitwise independent of
+// which block ran which item.  The arithmetic per (pair, point) is that of
+// fe_eval_f64_kernel: results equal fe_esp_fp64 up to the order of the part
+// sums.  The g-shell classes (7, 8) have their own queue and kernel instance.
 #pragma once
 #include "eval_f64.cuh"
 
@@ -19,28 +21,29 @@ struct FeBatchMolDev {
   const double* pts;
   double* out;
   int npts;
-  int nsplit;          // pair splits of this molecule
-  int ld;              // row length (points, padded to 32)
-  int nrows;           // rows of all kernel instances: nsplit * instances
-  long long base;      // its first partial row starts at partial + base (doubles)
-  long long pt0;       // first point of this molecule in the flattened point index
+  int ld;                  // row length (points, padded to 32)
+  int nrows;               // rows of all classes
+  int pad_;
+  int row0[FE_NCLASS];     // first row of class L
+  int nsplit[FE_NCLASS];   // parts of class L (0: class empty)
+  long long base;          // its first partial row starts at partial + base (doubles)
+  long long pt0;           // first point of this molecule in the flattened point index
 };
 
 struct FeBatchHdr {
   int n_mol;
-  int n_item;
-  int np;              // points per thread of the items' point blocks
-  int n_inst;          // kernel instances (1: classes 0..FE_LSPLIT, 2: also the rest)
+  int np;                  // points per thread of the items' point blocks
+  int n_item[2];           // items of the two queues (classes 0..FE_LSPLIT, the rest)
   long long total_pts;
-  long long off_mol;   // byte offsets within the descriptor
-  long long off_item;
+  long long off_mol;       // byte offsets within the descriptor
+  long long off_item[2];
 };
 
 struct FeBatchItem {
-  int mol, pblock, split, pad_;
+  int mol, pblock, cls, part;
 };
 
-template <int NP, int MINB, int LLO, int LHI, int INST>
+template <int NP, int MINB, int LLO, int LHI, int Q>
 __global__ void __launch_bounds__(128, MINB) fe_batch_f64_kernel(const unsigned char* __restrict__ desc,
                                                                  unsigned* counter,
                                                                  double* partial) {
@@ -51,7 +54,8 @@ __global__ void __launch_bounds__(128, MINB) fe_batch_f64_kernel(const unsigned 
   __shared__ int item_s;
   const FeBatchHdr* bh = reinterpret_cast<const FeBatchHdr*>(desc);
   const FeBatchMolDev* mols = reinterpret_cast<const FeBatchMolDev*>(desc + bh->off_mol);
-  const FeBatchItem* items = reinterpret_cast<const FeBatchItem*>(desc + bh->off_item);
+  const FeBatchItem* items = reinterpret_cast<const FeBatchItem*>(desc + bh->off_item[Q]);
+  const int n_item = bh->n_item[Q];
   const int tid = threadIdx.x;
   FeTilePipe pipe{nullptr, fe_c_tile64, fe_c_rec64, nullptr, 8, fe_smem, full_bar, &w};
   pipe.init_barriers();
@@ -59,9 +63,10 @@ __global__ void __launch_bounds__(128, MINB) fe_batch_f64_kernel(const unsigned 
     if (tid == 0) item_s = int(atomicAdd(counter, 1u));
     __syncthreads();
     const int it = item_s;
-    if (it >= bh->n_item) break;
+    if (it >= n_item) break;
     const FeBatchItem item = items[it];
-    const FeBatchMolDev m = mols[item.mol];
+    const FeBatchMolDev& m = mols[item.mol];
+    const int L = item.cls;
     const FeTableHdr* hdr = reinterpret_cast<const FeTableHdr*>(m.table);
     double cx[NP], cy[NP], cz[NP], acc[NP];
     const int p0 = item.pblock * (NT * NP) + tid;
@@ -75,7 +80,8 @@ __global__ void __launch_bounds__(128, MINB) fe_batch_f64_kernel(const unsigned 
     }
     pipe.table = m.table;
     pipe.off = hdr->off64;
-    pipe.begin(hdr, item.split, m.nsplit, LLO, LHI);
+    if (L >= LLO && L <= LHI) pipe.begin(hdr, item.part, m.nsplit[L], L, L);
+    else pipe.begin(hdr, 0, 1, 1, 0);                  // not this instance's class: no tiles
     const int total = w.total;
     bool ok = true;
     for (int i = 0; i < total; ++i) {
@@ -84,21 +90,20 @@ __global__ void __launch_bounds__(128, MINB) fe_batch_f64_kernel(const unsigned 
         ok = false;
         break;
       }
-      int L, first, n;
-      fe_item(w, fe_c_tile64, i, L, first, n);
+      int Lt, first, n;
+      fe_item(w, fe_c_tile64, i, Lt, first, n);
       const double* rec = reinterpret_cast<const double*>(pipe.stage(i));
-#define FE_CB(l) if (l >= LLO && l <= LHI && L == l) fe_tile_f64<(l >= LLO && l <= LHI ? l : LLO), NP>(rec, n, cx, cy, cz, acc);
+#define FE_CB(l) if (l >= LLO && l <= LHI && Lt == l) fe_tile_f64<(l >= LLO && l <= LHI ? l : LLO), NP>(rec, n, cx, cy, cz, acc);
       FE_CB(0) FE_CB(1) FE_CB(2) FE_CB(3) FE_CB(4) FE_CB(5) FE_CB(6) FE_CB(7) FE_CB(8)
 #undef FE_CB
-      if (L < LLO || L > LHI) fe_flag(FE_ST_BADCLASS);
       pipe.release(i);
     }
     if (!ok) return;               // the status word says why; outputs are not valid
+    if (L < LLO || L > LHI) fe_flag(FE_ST_BADCLASS);
 #pragma unroll
     for (int j = 0; j < NP; ++j) {
       const int p = p0 + j * NT;
-      if (p < m.npts)
-        partial[m.base + size_t(INST * m.nsplit + item.split) * m.ld + p] = acc[j];
+      if (p < m.npts) partial[m.base + size_t(m.row0[L] + item.part) * m.ld + p] = acc[j];
     }
     pipe.base += total;
     __syncthreads();               // w and item_s are rewritten by the next item
@@ -117,7 +122,7 @@ __global__ void fe_batch_reduce_kernel(const unsigned char* __restrict__ desc,
     const int mid = (lo + hi + 1) / 2;
     if (mols[mid].pt0 <= q) lo = mid; else hi = mid - 1;
   }
-  const FeBatchMolDev m = mols[lo];
+  const FeBatchMolDev& m = mols[lo];
   const int i = int(q - m.pt0);
   if (i >= m.npts) return;
   double e = 0.0;

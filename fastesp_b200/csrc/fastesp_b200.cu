@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstddef>
@@ -1007,14 +1008,15 @@ int fe_esp_adjoint(const fe_plan* p, const void* d_plan, const void* d_table,
 // Batched evaluation
 // ---------------------------------------------------------------------------
 struct fe_batch {
-  int np = 2, n_inst = 1;
+  int np = 2;
   int grid[2] = {1, 1};
   std::vector<FeBatchMolDev> mols;
-  std::vector<FeBatchItem> items;
+  std::vector<FeBatchItem> items[2];     // classes 0..FE_LSPLIT, the g-shell classes
   long long total_pts = 0;
   size_t partial_doubles = 0;
   size_t desc_bytes = 0, ws_bytes = 0;
-  size_t off_mol = 0, off_item = 0;
+  size_t off_mol = 0, off_item[2] = {0, 0};
+  int n_items() const { return int(items[0].size() + items[1].size()); }
 };
 
 namespace {
@@ -1073,10 +1075,10 @@ int fe_batch_create(const fe_batch_mol* in, int n_mol, const fe_batch_shape* sha
   auto* b = new fe_batch();
   b->np = np;
   const int ppb = 128 * np;
-  std::vector<double> work(n_mol, 0.0);   // FLOPs per point of each molecule
-  std::vector<int> npairs(n_mol, 0);
+  std::vector<std::array<int, FE_NCLASS>> cnt(n_mol);
   double total = 0.0;
   for (int m = 0; m < n_mol; ++m) {
+    cnt[m].fill(0);
     if (in[m].n_pts < 0 || (in[m].n_pts > 0 && (!in[m].d_table || !in[m].d_pts || !in[m].d_out))) {
       delete b;
       return fail(FE_ERR_ARG, "fe_batch_create: molecule %d: bad buffers", m);
@@ -1090,15 +1092,16 @@ int fe_batch_create(const fe_batch_mol* in, int n_mol, const fe_batch_shape* sha
       return fail(FE_ERR_ARG, "fe_batch_create: molecule %d: not a pair table", m);
     }
     for (int L = 0; L < FE_NCLASS; ++L) {
-      work[m] += h.count[L] * pair_point_flops(L);
-      npairs[m] += h.count[L];
-      if (L > FE_LSPLIT && h.count[L] > 0) b->n_inst = 2;
+      cnt[m][L] = h.count[L];
+      total += double(h.count[L]) * pair_point_flops(L) * in[m].n_pts;
     }
-    total += work[m] * in[m].n_pts;
   }
-  // pair splits: items of about equal cost, ``waves`` items per resident block
+  // parts per (molecule, class): items of about equal cost, ``waves`` items per
+  // resident block
   const double target_items = double(waves) * occ0 * sm_count();
   const double item_cost = std::max(1.0, total / target_items);
+  struct Keyed { FeBatchItem it; double cost; };
+  std::vector<Keyed> q[2];
   long long base = 0, pt0 = 0;
   for (int m = 0; m < n_mol; ++m) {
     FeBatchMolDev d{};
@@ -1106,38 +1109,50 @@ int fe_batch_create(const fe_batch_mol* in, int n_mol, const fe_batch_shape* sha
     d.pts = in[m].d_pts;
     d.out = in[m].d_out;
     d.npts = in[m].n_pts;
-    int ns = int(std::ceil(ppb * work[m] / item_cost));
-    ns = std::max(1, std::min({ns, 256, std::max(1, npairs[m] / 32)}));
-    d.nsplit = ns;
     d.ld = (std::max(d.npts, 1) + 31) & ~31;
-    d.nrows = ns * b->n_inst;
+    int rows = 0;
+    for (int L = 0; L < FE_NCLASS; ++L) {
+      d.row0[L] = rows;
+      d.nsplit[L] = 0;
+      if (cnt[m][L] == 0 || d.npts == 0) continue;
+      const double w = double(cnt[m][L]) * pair_point_flops(L);      // per point
+      int ns = int(std::ceil(ppb * w / item_cost));
+      ns = std::max(1, std::min({ns, 256, std::max(1, cnt[m][L] / 32)}));
+      d.nsplit[L] = ns;
+      rows += ns;
+    }
+    d.nrows = rows;
     d.base = base;
     d.pt0 = pt0;
     if (d.npts > 0) {
       base += (long long)d.nrows * d.ld;
       pt0 += d.npts;
       const int nb = (d.npts + ppb - 1) / ppb;
-      for (int pb = 0; pb < nb; ++pb)
-        for (int s = 0; s < ns; ++s) b->items.push_back(FeBatchItem{m, pb, s, 0});
+      for (int L = 0; L < FE_NCLASS; ++L)
+        for (int pb = 0; pb < nb && d.nsplit[L] > 0; ++pb) {
+          const int pts = std::min(ppb, d.npts - pb * ppb);
+          const double c = double(pts) * cnt[m][L] * pair_point_flops(L) / d.nsplit[L];
+          for (int s2 = 0; s2 < d.nsplit[L]; ++s2)
+            q[L > FE_LSPLIT].push_back(Keyed{FeBatchItem{m, pb, L, s2}, c});
+        }
     }
     b->mols.push_back(d);
   }
-  // largest first (stable, so the order is deterministic)
-  auto cost = [&](const FeBatchItem& it) {
-    const FeBatchMolDev& d = b->mols[it.mol];
-    const int pts = std::min(ppb, d.npts - it.pblock * ppb);
-    return double(pts) * work[it.mol] / d.nsplit;
-  };
-  std::stable_sort(b->items.begin(), b->items.end(),
-                   [&](const FeBatchItem& x, const FeBatchItem& y) { return cost(x) > cost(y); });
+  // class-major, largest first within a class (stable: deterministic order)
+  for (int k = 0; k < 2; ++k) {
+    std::stable_sort(q[k].begin(), q[k].end(), [](const Keyed& x, const Keyed& y) {
+      return x.it.cls != y.it.cls ? x.it.cls < y.it.cls : x.cost > y.cost;
+    });
+    for (const Keyed& e : q[k]) b->items[k].push_back(e.it);
+  }
   b->total_pts = pt0;
   b->partial_doubles = size_t(base);
-  const int nit = int(b->items.size());
-  b->grid[0] = std::max(1, std::min(nit, occ0 * sm_count()));
-  b->grid[1] = std::max(1, std::min(nit, occ1 * sm_count()));
+  b->grid[0] = std::max(1, std::min(int(b->items[0].size()), occ0 * sm_count()));
+  b->grid[1] = std::max(1, std::min(int(b->items[1].size()), occ1 * sm_count()));
   b->off_mol = align256(sizeof(FeBatchHdr));
-  b->off_item = align256(b->off_mol + b->mols.size() * sizeof(FeBatchMolDev));
-  b->desc_bytes = align256(b->off_item + b->items.size() * sizeof(FeBatchItem));
+  b->off_item[0] = align256(b->off_mol + b->mols.size() * sizeof(FeBatchMolDev));
+  b->off_item[1] = align256(b->off_item[0] + b->items[0].size() * sizeof(FeBatchItem));
+  b->desc_bytes = align256(b->off_item[1] + b->items[1].size() * sizeof(FeBatchItem));
   b->ws_bytes = kBatchCounterBytes + align256(b->partial_doubles * sizeof(double));
   *out = b;
   return FE_OK;
@@ -1149,7 +1164,7 @@ int fe_batch_sizes(const fe_batch* b, size_t* desc_bytes, size_t* ws_bytes, int*
   if (!b) return fail(FE_ERR_ARG, "fe_batch_sizes: null batch");
   if (desc_bytes) *desc_bytes = b->desc_bytes;
   if (ws_bytes) *ws_bytes = b->ws_bytes;
-  if (n_items) *n_items = int(b->items.size());
+  if (n_items) *n_items = b->n_items();
   return FE_OK;
 }
 
@@ -1160,15 +1175,18 @@ int fe_batch_upload(const fe_batch* b, void* d_desc, size_t desc_bytes, cudaStre
   std::vector<unsigned char> h(b->desc_bytes, 0);
   FeBatchHdr hdr{};
   hdr.n_mol = int(b->mols.size());
-  hdr.n_item = int(b->items.size());
   hdr.np = b->np;
-  hdr.n_inst = b->n_inst;
   hdr.total_pts = b->total_pts;
   hdr.off_mol = static_cast<long long>(b->off_mol);
-  hdr.off_item = static_cast<long long>(b->off_item);
+  for (int k = 0; k < 2; ++k) {
+    hdr.n_item[k] = int(b->items[k].size());
+    hdr.off_item[k] = static_cast<long long>(b->off_item[k]);
+  }
   memcpy(h.data(), &hdr, sizeof hdr);
   if (!b->mols.empty()) memcpy(h.data() + b->off_mol, b->mols.data(), b->mols.size() * sizeof(FeBatchMolDev));
-  if (!b->items.empty()) memcpy(h.data() + b->off_item, b->items.data(), b->items.size() * sizeof(FeBatchItem));
+  for (int k = 0; k < 2; ++k)
+    if (!b->items[k].empty())
+      memcpy(h.data() + b->off_item[k], b->items[k].data(), b->items[k].size() * sizeof(FeBatchItem));
   FE_CUDA(cudaMemcpyAsync(d_desc, h.data(), h.size(), cudaMemcpyHostToDevice, st));
   FE_CUDA(cudaStreamSynchronize(st));   // h is a local buffer
   return FE_OK;
@@ -1176,7 +1194,7 @@ int fe_batch_upload(const fe_batch* b, void* d_desc, size_t desc_bytes, cudaStre
 
 int fe_batch_run(const fe_batch* b, const void* d_desc, void* d_ws, size_t ws_bytes, cudaStream_t st) {
   if (!b || !d_desc) return fail(FE_ERR_ARG, "fe_batch_run: null argument");
-  if (b->items.empty()) return FE_OK;
+  if (b->n_items() == 0) return FE_OK;
   if (!d_ws || ws_bytes < b->ws_bytes) return fail(FE_ERR_SIZE, "fe_batch_run: workspace too small (need %zu bytes)", b->ws_bytes);
   const void* k0 = nullptr;
   const void* k1 = nullptr;
@@ -1191,9 +1209,11 @@ int fe_batch_run(const fe_batch* b, const void* d_desc, void* d_ws, size_t ws_by
   FE_CUDA(cudaMemsetAsync(counter, 0, kBatchCounterBytes, st));
   const int smem = FE_NSTAGE * FE_STAGE_BYTES;
   unsigned* c1 = counter + 32;
-  void* a0[] = {&desc, &counter, &partial};
-  FE_CUDA(cudaLaunchKernel(k0, dim3(b->grid[0]), dim3(128), a0, smem, st));
-  if (b->n_inst == 2) {
+  if (!b->items[0].empty()) {
+    void* a0[] = {&desc, &counter, &partial};
+    FE_CUDA(cudaLaunchKernel(k0, dim3(b->grid[0]), dim3(128), a0, smem, st));
+  }
+  if (!b->items[1].empty()) {
     void* a1[] = {&desc, &c1, &partial};
     FE_CUDA(cudaLaunchKernel(k1, dim3(b->grid[1]), dim3(128), a1, smem, st));
   }
