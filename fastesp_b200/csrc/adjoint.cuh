@@ -20,8 +20,8 @@
 //   fe_field_f64_kernel     point-parallel like the FP64 evaluator; four
 //                           partial planes (V_el and its three derivatives)
 //   fe_field_reduce_kernel  fixed-order sum of the planes, nuclear terms, w_i
-//   fe_adj_moments_kernel   one thread per (pair, term chunk), all points
-//                           streamed through shared memory
+//   fe_adj_moments_kernel   one block per (pair, term chunk), its threads
+//                           over the points, moments reduced in a fixed order
 //   fe_adj_pair_kernel      one thread per pair: the Hermite coefficients are
 //                           recomputed (never stored), lambda, dL/dW per component
 //   fe_adj_ranges_kernel,   deterministic segmented sum of dL/dW over each
@@ -155,7 +155,6 @@ __global__ void fe_field_reduce_kernel(const unsigned char* table, const double*
 // adjoint with respect to the density
 // ---------------------------------------------------------------------------
 #define FE_ADJ_THREADS 128
-#define FE_ADJ_PTILE 256     // points staged per shared-memory round
 
 struct FeAdjArgs {
   const unsigned char* table;
@@ -182,49 +181,52 @@ struct FeAdjArgs {
 };
 
 // mom[pair][k] = sum_i w_i R_i^a_k F_m_k(p R_i^2) for the terms of chunk C.
+// One block per pair (and chunk): the pair is warp-uniform, as in the forward
+// evaluator, so the lanes -- points i = tid, tid + 128, ... -- share the Boys
+// branch of nearby points; each thread accumulates its points' moments in
+// registers, then a fixed butterfly per warp and a fixed sum over the warps
+// (deterministic) give the pair's moments.
 template <int L, int C>
 __global__ void __launch_bounds__(FE_ADJ_THREADS) fe_adj_moments_kernel(const FeAdjArgs a) {
   constexpr int K0 = fe_mom_k0[L][C], N = fe_mom_k1[L][C] - fe_mom_k0[L][C];
   constexpr int NTERM = fe_class_nterm[L];
-  __shared__ double sx[FE_ADJ_PTILE], sy[FE_ADJ_PTILE], sz[FE_ADJ_PTILE], sw[FE_ADJ_PTILE];
+  constexpr int NW = FE_ADJ_THREADS / 32;
+  __shared__ double red[NW][N];
   const FeTableHdr* hdr = reinterpret_cast<const FeTableHdr*>(a.table);
-  const int count = hdr->count[L];
-  const int i0 = blockIdx.x * FE_ADJ_THREADS;
-  if (i0 >= count) return;                          // the whole block
-  const int tid = threadIdx.x;
-  const int i = min(i0 + tid, count - 1);
+  const int i = blockIdx.x;
+  if (i >= hdr->count[L]) return;                  // the whole block
+  const int tid = threadIdx.x, lane = tid & 31, wi = tid >> 5;
   const double* rec = reinterpret_cast<const double*>(a.table + hdr->off64[L]) +
                       size_t(i) * fe_class_rec64[L];
   const double pe = rec[0], px = rec[1], py = rec[2], pz = rec[3];
   double acc[N];
 #pragma unroll
   for (int k = 0; k < N; ++k) acc[k] = 0.0;
-  for (int c0 = 0; c0 < a.npts; c0 += FE_ADJ_PTILE) {
-    const int m = min(FE_ADJ_PTILE, a.npts - c0);
-    __syncthreads();
-    for (int q = tid; q < m; q += FE_ADJ_THREADS) {
-      sx[q] = a.pts[3 * (c0 + q)];
-      sy[q] = a.pts[3 * (c0 + q) + 1];
-      sz[q] = a.pts[3 * (c0 + q) + 2];
-      sw[q] = a.w[c0 + q];
-    }
-    __syncthreads();
 #pragma unroll 1
-    for (int j = 0; j < m; ++j) {
-      const double x = sx[j] - px, y = sy[j] - py, z = sz[j] - pz;
-      const double T = pe * fma(x, x, fma(y, y, z * z));
-      double F[L + 1];
-      fe_boys_f64<L>(T, F);
-      const double wj = sw[j];
+  for (int q = tid; q < a.npts; q += FE_ADJ_THREADS) {
+    const double x = a.pts[3 * q] - px, y = a.pts[3 * q + 1] - py, z = a.pts[3 * q + 2] - pz;
+    const double T = pe * fma(x, x, fma(y, y, z * z));
+    double F[L + 1];
+    fe_boys_f64<L>(T, F);
+    const double wq = a.w[q];
 #pragma unroll
-      for (int q = 0; q <= L; ++q) F[q] *= wj;
-      fe_mom<L, C, double>(x, y, z, F, acc);
-    }
+    for (int m = 0; m <= L; ++m) F[m] *= wq;
+    fe_mom<L, C, double>(x, y, z, F, acc);
   }
-  if (i0 + tid < count) {
-    double* out = a.mom + a.mom_off[L] + size_t(i) * NTERM + K0;
 #pragma unroll
-    for (int k = 0; k < N; ++k) out[k] = acc[k];
+  for (int k = 0; k < N; ++k) {
+    double v = acc[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[wi][k] = v;
+  }
+  __syncthreads();
+  double* out = a.mom + a.mom_off[L] + size_t(i) * NTERM + K0;
+  for (int k = tid; k < N; k += FE_ADJ_THREADS) {
+    double v = red[0][k];
+#pragma unroll
+    for (int u = 1; u < NW; ++u) v += red[u][k];
+    out[k] = v;
   }
 }
 

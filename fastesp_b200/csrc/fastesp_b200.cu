@@ -894,9 +894,7 @@ AdjLayout adj_layout(const fe_plan* p, int n_pts) {
 template <int L, int C>
 int launch_moments(const FeAdjArgs& a, int cap, cudaStream_t st) {
   if constexpr (C < fe_mom_nchunk[L]) {
-    if (cap > 0)
-      fe_adj_moments_kernel<L, C><<<(cap + FE_ADJ_THREADS - 1) / FE_ADJ_THREADS, FE_ADJ_THREADS, 0,
-                                    st>>>(a);
+    if (cap > 0) fe_adj_moments_kernel<L, C><<<cap, FE_ADJ_THREADS, 0, st>>>(a);
     FE_CUDA(cudaGetLastError());
     return launch_moments<L, C + 1>(a, cap, st);
   } else {
