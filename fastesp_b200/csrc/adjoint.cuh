@@ -91,7 +91,10 @@ __global__ void __launch_bounds__(NT, MINB) fe_field_f64_kernel(const FeFieldArg
     for (int c = 0; c < 4; ++c) acc[c][j] = 0.0;
   }
   FeTilePipe pipe{a.table, fe_c_tile64, fe_c_rec64, hdr->off64, 8, fe_smem, full_bar, &w};
-  pipe.start(hdr, split, a.nsplit, LLO, LHI);
+  int Lrow, part, nparts;
+  fe_class_rows(hdr, LLO, LHI, a.nsplit, split, Lrow, part, nparts);
+  if (Lrow >= 0) pipe.start(hdr, part, nparts, Lrow, Lrow);
+  else pipe.start(hdr, 0, 1, 1, 0);                     // idle row: no tiles
   const int total = w.total;
   for (int i = 0; i < total; ++i) {
     if (!pipe.wait(i)) {

@@ -822,8 +822,10 @@ FieldGeom field_geom(int npts) {
   const int ppb = kEvalThreads * kNPField;
   g.nblk_x = (npts + ppb - 1) / ppb;
   const int target = 8 * kMinBField * sm_count();
-  g.split[0] = std::max(1, std::min(256, (target + g.nblk_x - 1) / std::max(1, g.nblk_x)));
-  g.split[1] = std::max(1, std::min(8, sm_count() / std::max(1, g.nblk_x)));
+  // at least one grid row per class of each instance's range (fe_class_rows)
+  g.split[0] = std::max(FE_LSPLIT + 1,
+                        std::min(256, (target + g.nblk_x - 1) / std::max(1, g.nblk_x)));
+  g.split[1] = std::max(FE_NCLASS - 1 - FE_LSPLIT, std::min(8, sm_count() / std::max(1, g.nblk_x)));
   g.ld = (npts + 31) & ~31;
   return g;
 }
