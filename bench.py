@@ -358,9 +358,10 @@ def _median_ms(fn, reps, warm=2, flush=None):
     return statistics.median(ts)
 
 
-def run_extras(args, dev, flush):
+def run_extras(args, dev, flush, which=("grid", "adjoint", "batch")):
     """Grid sweep (mixed vs FP64 on a cubic grid), the adjoint on the 20-atom
-    l<=2 system, and the 64-molecule batch against 64 plain launches."""
+    l<=2 system and at the headline size, and the 64-molecule batch against 64
+    plain launches (``which`` selects)."""
     import torch
     from fastesp_b200 import build_table, synth
     from fastesp_b200.batch import BatchESP, separate_launches
@@ -368,7 +369,7 @@ def run_extras(args, dev, flush):
     wfn, basis, P, _ = synth.load_workload("frag54", 10, seed=0)
     P_d = torch.as_tensor(P, device=dev)
     sweep = []
-    for n in args.grid_points:
+    for n in (args.grid_points if "grid" in which else []):
         pts = torch.as_tensor(synth.cubic_grid_points(wfn.coords, n, seed=2), device=dev)
         tb = _median_ms(lambda: build_table(wfn, basis, P_d, pts), 3, warm=1, flush=flush)
         tab = build_table(wfn, basis, P_d, pts)
@@ -384,54 +385,57 @@ def run_extras(args, dev, flush):
                       "mixed_max_abs_err": float(d.max()), "mixed_rms_err": float(d.pow(2).mean().sqrt()),
                       "fp64_routed_pair_warp_evals": n64})
         del tab, pts, v64, vmx
-    out["grid_sweep"] = {"workload": "frag54 on a cubic grid of 0.2 Bohr spacing, 4 Bohr margin, "
-                                     "points within 0.3 Bohr of a nucleus dropped; errors of the "
-                                     "mixed path against the FP64 path", "runs": sweep}
-    # adjoint: 20 atoms l<=2, 500 surface points, L = 0.5 ||V - V_target||^2
-    w3, b3, P3, p3 = synth.load_workload("adjoint20", 500, seed=0)
-    P3d = torch.as_tensor(P3, device=dev)
-    p3d = torch.as_tensor(p3, device=dev)
-    rng = np.random.default_rng(7)
-    E = rng.normal(0.0, 1e-3, P3.shape)
-    vt = build_table(w3, b3, P3d + torch.as_tensor(0.5 * (E + E.T), device=dev), p3d).esp(p3d)
-    t3 = build_table(w3, b3, P3d, p3d)
-    wv = t3.esp(p3d) - vt
-    t_fwd = _median_ms(lambda: build_table(w3, b3, P3d, p3d).esp(p3d), 5)
-    t_adj = _median_ms(lambda: t3.adjoint(p3d, wv), 5)
-    t_fld = _median_ms(lambda: t3.adjoint(p3d, wv, density=False), 5)
-    out["adjoint"] = {"workload": f"adjoint20: 20 atoms, l<=2, {b3.n} Cartesian functions, 500 points",
-                      "pairs": t3.n_pairs, "forward_ms": t_fwd, "adjoint_dP_dC_ms": t_adj,
-                      "adjoint_dC_only_ms": t_fld}
-    # the same adjoint at the headline size (54 atoms, l<=3, 30000 points)
-    pts54 = torch.as_tensor(synth.vdw_surface_points(wfn.symbols, wfn.coords, 30000, seed=1),
-                            device=dev)
-    t54 = build_table(wfn, basis, P_d, pts54)
-    w54 = torch.linspace(-1.0, 1.0, pts54.shape[0], dtype=torch.float64, device=dev)
-    out["adjoint"]["frag54_30000"] = {
-        "pairs": t54.n_pairs,
-        "forward_fp64_ms": _median_ms(lambda: t54.esp(pts54), 3, warm=1),
-        "adjoint_dP_dC_ms": _median_ms(lambda: t54.adjoint(pts54, w54), 3, warm=1),
-        "adjoint_dC_only_ms": _median_ms(lambda: t54.adjoint(pts54, w54, density=False), 3, warm=1)}
-    del t54, pts54
-    # batch: 64 uneven molecules
-    mols = synth.batch_workload(64, seed=0)
-    tabs, pts = [], []
-    for wfn_, basis_, P_, p_ in mols:
-        pd = torch.as_tensor(p_, device=dev)
-        tabs.append(build_table(wfn_, basis_, torch.as_tensor(P_, device=dev), pd))
-        pts.append(pd)
-    b = BatchESP(tabs, pts)
-    _, run_sep = separate_launches(tabs, pts)
-    tbat = _median_ms(b.run, 10, flush=flush)
-    tsep = _median_ms(run_sep, 10, flush=flush)
-    err = max(float((x - y).abs().max()) for x, y in zip(b.run(), run_sep()))
-    npts = sum(int(p.shape[0]) for p in pts)
-    out["batch"] = {"workload": "64 molecules, 5-60 atoms, l<=2, 200-5000 surface points each",
-                    "points": npts, "pairs": sum(t.n_pairs for t in tabs),
-                    "batched_graph_ms": tbat, "separate_launches_ms": tsep,
-                    "speedup": tsep / tbat, "points_per_s": npts / (tbat * 1e-3),
-                    "shape": list(b.shape), "items": b.n_items, "max_abs_diff": err,
-                    "autotune_ms": {f"{k[0]}x{k[1]}": v for k, v in (b.tuning or {}).items()}}
+    if "grid" in which:
+        out["grid_sweep"] = {"workload": "frag54 on a cubic grid of 0.2 Bohr spacing, 4 Bohr margin, "
+                                         "points within 0.3 Bohr of a nucleus dropped; errors of the "
+                                         "mixed path against the FP64 path", "runs": sweep}
+    if "adjoint" in which:
+        # adjoint: 20 atoms l<=2, 500 surface points, L = 0.5 ||V - V_target||^2
+        w3, b3, P3, p3 = synth.load_workload("adjoint20", 500, seed=0)
+        P3d = torch.as_tensor(P3, device=dev)
+        p3d = torch.as_tensor(p3, device=dev)
+        rng = np.random.default_rng(7)
+        E = rng.normal(0.0, 1e-3, P3.shape)
+        vt = build_table(w3, b3, P3d + torch.as_tensor(0.5 * (E + E.T), device=dev), p3d).esp(p3d)
+        t3 = build_table(w3, b3, P3d, p3d)
+        wv = t3.esp(p3d) - vt
+        t_fwd = _median_ms(lambda: build_table(w3, b3, P3d, p3d).esp(p3d), 5)
+        t_adj = _median_ms(lambda: t3.adjoint(p3d, wv), 5)
+        t_fld = _median_ms(lambda: t3.adjoint(p3d, wv, density=False), 5)
+        out["adjoint"] = {"workload": f"adjoint20: 20 atoms, l<=2, {b3.n} Cartesian functions, 500 points",
+                          "pairs": t3.n_pairs, "forward_ms": t_fwd, "adjoint_dP_dC_ms": t_adj,
+                          "adjoint_dC_only_ms": t_fld}
+        # the same adjoint at the headline size (54 atoms, l<=3, 30000 points)
+        pts54 = torch.as_tensor(synth.vdw_surface_points(wfn.symbols, wfn.coords, 30000, seed=1),
+                                device=dev)
+        t54 = build_table(wfn, basis, P_d, pts54)
+        w54 = torch.linspace(-1.0, 1.0, pts54.shape[0], dtype=torch.float64, device=dev)
+        out["adjoint"]["frag54_30000"] = {
+            "pairs": t54.n_pairs,
+            "forward_fp64_ms": _median_ms(lambda: t54.esp(pts54), 3, warm=1),
+            "adjoint_dP_dC_ms": _median_ms(lambda: t54.adjoint(pts54, w54), 3, warm=1),
+            "adjoint_dC_only_ms": _median_ms(lambda: t54.adjoint(pts54, w54, density=False), 3, warm=1)}
+        del t54, pts54
+    if "batch" in which:
+        # batch: 64 uneven molecules
+        mols = synth.batch_workload(64, seed=0)
+        tabs, pts = [], []
+        for wfn_, basis_, P_, p_ in mols:
+            pd = torch.as_tensor(p_, device=dev)
+            tabs.append(build_table(wfn_, basis_, torch.as_tensor(P_, device=dev), pd))
+            pts.append(pd)
+        b = BatchESP(tabs, pts)
+        _, run_sep = separate_launches(tabs, pts)
+        tbat = _median_ms(b.run, 10, flush=flush)
+        tsep = _median_ms(run_sep, 10, flush=flush)
+        err = max(float((x - y).abs().max()) for x, y in zip(b.run(), run_sep()))
+        npts = sum(int(p.shape[0]) for p in pts)
+        out["batch"] = {"workload": "64 molecules, 5-60 atoms, l<=2, 200-5000 surface points each",
+                        "points": npts, "pairs": sum(t.n_pairs for t in tabs),
+                        "batched_graph_ms": tbat, "separate_launches_ms": tsep,
+                        "speedup": tsep / tbat, "points_per_s": npts / (tbat * 1e-3),
+                        "shape": list(b.shape), "items": b.n_items, "max_abs_diff": err,
+                        "autotune_ms": {f"{k[0]}x{k[1]}": v for k, v in (b.tuning or {}).items()}}
     return out
 
 
@@ -564,12 +568,20 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the grid sweep, adjoint and batch measurements")
     ap.add_argument("--grid-points", type=int, nargs="*", default=[100000, 1000000])
+    ap.add_argument("--only", choices=["grid", "adjoint", "batch"], default=None,
+                    help="run one of the extra measurements alone and print its JSON")
     ap.add_argument("--eval-only", action="store_true",
                     help="time only the two evaluators (short run for profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.only:
+        import torch
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+        print(json.dumps({"only": args.only, **run_extras(args, dev, flush, which=(args.only,))}))
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
