@@ -73,29 +73,43 @@ FE_DEV void fe_boys_f64(const double T, double (&F)[M + 1]) {
   }
 }
 
-// FP32 Boys vector for the mixed-precision evaluator.  Asymptotic above
-// fe_boys32_asym_T[M] (2e-8 relative); below it a 6-term Taylor expansion
-// about the nearest point of a 1/4 grid over 0 <= T < 32 held in shared
-// memory (``grid``, truncation below 6e-9 relative), then the downward
-// recursion.  The FP32 thresholds of orders <= 6 lie below 32, so the common
-// classes have only these two branches; for higher orders the stretch from 32
-// to the threshold uses the upward recursion from erf.  ``rt`` is T^-1/2,
-// which the caller already has.
+// FP32 Boys vectors for the mixed-precision evaluator, in the scaled form
+// F^_m(T) = F_m(T) / s_m, s_m = (sqrt(pi)/2) (2m-1)!!/2^m (the FP32 records
+// carry s_m folded into their coefficients, in FP64).  In that form
+//  * the asymptotic branch is F^_m = T^-(m+1/2): F^_0 = rt, F^_(m+1) = F^_m / T;
+//  * the downward recursion is F^_(m-1) = T F^_m + E_m with E_m = e^-T / (2 s_m),
+//    E_(m-1) = E_m (2m-1)/2; the upward one F^_(m+1) = (F^_m - E_(m+1)) / T;
+// every constant in them is exact in FP32 (E_M takes 1/(2 s_M) as a float
+// hi/lo pair), so no rounded constant biases all pairs alike.
+// Asymptotic above fe_boys32_asym_T[M] (2e-8 relative); below it a 6-term
+// Taylor expansion about the nearest point of a 1/4 grid over 0 <= T < 32 held
+// in shared memory (``grid``, truncation below 6e-9 relative), then the
+// downward recursion.  The FP32 thresholds of orders <= 6 lie below 32, so the
+// common classes have only these two branches; for higher orders the stretch
+// from 32 to the threshold uses the upward recursion from erf.  ``rt`` is
+// T^-1/2, which the caller already has.  This scalar form reads the unscaled
+// rows fe_boys_grid32 and scales F_M by 1/s_M (a float hi/lo pair).
 template <int M>
 FE_DEV void fe_boys_f32(const float T, const float rt, const float* __restrict__ grid,
                         float (&F)[M + 1]) {
   constexpr float t_asym = fe_boys32_asym_T[M];
+  constexpr float kh = fe_boys32_kappa_hi[M], kl = fe_boys32_kappa_lo[M];
+  constexpr float sh = fe_boys32_sinv_hi[M], sl = fe_boys32_sinv_lo[M];
   if (T >= t_asym) {
-    const float h = 0.5f * rt * rt;
-    F[0] = float(FE_SQRT_PI_2) * rt;
+    const float it = rt * rt;
+    F[0] = rt;
 #pragma unroll
-    for (int m = 0; m < M; ++m) F[m + 1] = F[m] * (float(2 * m + 1) * h);
+    for (int m = 0; m < M; ++m) F[m + 1] = F[m] * it;
   } else if (t_asym > FE_BOYS32_GRID_TMAX && T >= FE_BOYS32_GRID_TMAX) {
-    const float h = 0.5f * rt * rt;
+    const float it = rt * rt;
     const float e = __expf(-T);
-    F[0] = float(FE_SQRT_PI_2) * rt * erff(T * rt);
+    float E[M + 1];
+    E[M] = fmaf(e, kh, e * kl);
 #pragma unroll
-    for (int m = 0; m < M; ++m) F[m + 1] = fmaf(float(2 * m + 1), F[m], -e) * h;
+    for (int m = M; m > 1; --m) E[m - 1] = E[m] * (float(2 * m - 1) * 0.5f);
+    F[0] = rt * erff(T * rt);
+#pragma unroll
+    for (int m = 0; m < M; ++m) F[m + 1] = (F[m] - E[m + 1]) * it;
   } else {
     const int i = __float2int_rn(T * FE_BOYS32_GRID_INV_H);
     const float d = -(T - float(i) * FE_BOYS32_GRID_H);
@@ -103,33 +117,37 @@ FE_DEV void fe_boys_f32(const float T, const float rt, const float* __restrict__
     float f = row[FE_BOYS32_TAYLOR_K - 1];
 #pragma unroll
     for (int k = FE_BOYS32_TAYLOR_K - 2; k >= 0; --k) f = fmaf(f, d * (1.0f / float(k + 1)), row[k]);
-    F[M] = f;
+    F[M] = fmaf(f, sh, f * sl);
     const float e = __expf(-T);
-    const float t2 = T + T;
+    float E = fmaf(e, kh, e * kl);
 #pragma unroll
-    for (int m = M; m > 0; --m) F[m - 1] = fmaf(t2, F[m], e) * (1.0f / float(2 * m - 1));
+    for (int m = M; m > 0; --m) {
+      F[m - 1] = fmaf(T, F[m], E);
+      E = E * (float(2 * m - 1) * 0.5f);
+    }
   }
 }
 
-// Packed FP32 Boys vectors of two arguments (one per float2 lane), for the
-// orders whose FP32 asymptotic threshold lies below the grid's end (M <= 6):
-// the tabulated and the asymptotic branch only.  Each lane gets what
-// fe_boys_f32 gives it (the same operations lane by lane); when the lanes fall
-// in different branches both are computed and each lane keeps its own.
-// ``grid`` holds the per-order scaled rows fe_boys_grid32s (F_(M+k)/k!), so the
-// Taylor polynomial is evaluated in d directly.
+// Packed scaled FP32 Boys vectors of two arguments (one per float2 lane), for
+// the orders whose FP32 asymptotic threshold lies below the grid's end
+// (M <= 6): the tabulated and the asymptotic branch only.  Each lane gets what
+// fe_boys_f32 would give it with the scaled rows; when the lanes fall in
+// different branches both are computed and each lane keeps its own.  ``grid``
+// holds the per-order scaled rows fe_boys_grid32s (F_(M+k)/(k! s_M)), so the
+// Taylor polynomial of F^_M is evaluated in d directly.
 template <int M>
 FE_DEV void fe_boys_f32x2(const float2 T, const float2 rt, const float* __restrict__ grid,
                           float2 (&F)[M + 1]) {
   constexpr float t_asym = fe_boys32_asym_T[M];
+  constexpr float kh = fe_boys32_kappa_hi[M], kl = fe_boys32_kappa_lo[M];
   static_assert(fe_boys32_asym_T[M] <= FE_BOYS32_GRID_TMAX, "two-branch form only");
   const bool ax = T.x >= t_asym, ay = T.y >= t_asym;
   float2 A[M + 1], G[M + 1];
   if (ax || ay) {
-    const float2 h = fe_f2(0.5f) * rt * rt;
-    A[0] = fe_f2(float(FE_SQRT_PI_2)) * rt;
+    const float2 it = rt * rt;
+    A[0] = rt;
 #pragma unroll
-    for (int m = 0; m < M; ++m) A[m + 1] = A[m] * (fe_f2(float(2 * m + 1)) * h);
+    for (int m = 0; m < M; ++m) A[m + 1] = A[m] * it;
   }
   if (!(ax && ay)) {
     // a lane in the asymptotic range reads a clamped, in-range row; its result is dropped
@@ -144,9 +162,12 @@ FE_DEV void fe_boys_f32x2(const float2 T, const float2 rt, const float* __restri
     for (int k = FE_BOYS32_TAYLOR_K - 2; k >= 0; --k) f = fe_fma(f, d, make_float2(rx[k], ry[k]));
     G[M] = f;
     const float2 e = make_float2(__expf(-T.x), __expf(-T.y));
-    const float2 t2 = T + T;
+    float2 E = fe_fma(e, fe_f2(kh), e * fe_f2(kl));
 #pragma unroll
-    for (int m = M; m > 0; --m) G[m - 1] = fe_fma(t2, G[m], e) * fe_f2(1.0f / float(2 * m - 1));
+    for (int m = M; m > 0; --m) {
+      G[m - 1] = fe_fma(T, G[m], E);
+      if (m > 1) E = E * fe_f2(float(2 * m - 1) * 0.5f);
+    }
   }
   if (ax && ay) {
 #pragma unroll

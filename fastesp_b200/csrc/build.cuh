@@ -552,8 +552,26 @@ __global__ void fe_make_f32_kernel(unsigned char* table) {
     split(r[4], o[8], o[9]);
     o[10] = float(r[5]);                 // K * bound (+inf when unknown)
     o[11] = float(1.0 / sqrt(r[0]));     // p^-1/2
-    for (int k = 0; k < NT; ++k) o[12 + 2 * k] = o[13 + 2 * k] = float(r[6 + k]);
-    for (int k = 12 + 2 * NT; k < R32; ++k) o[k] = 0.0f;
+    // coefficients times s_m = (sqrt(pi)/2) (2m-1)!!/2^m, in FP64: the FP32
+    // evaluator's Boys vector is F_m / s_m (boys.cuh)
+    double sm[FE_NCLASS];
+    sm[0] = FE_SQRT_PI_2;
+    for (int m = 1; m <= L; ++m) sm[m] = sm[m - 1] * (0.5 * double(2 * m - 1));
+    const int c0 = fe_route_off[L];
+    for (int k = 0; k < NT; ++k)
+      o[12 + 2 * k] = o[13 + 2 * k] = float(r[6 + k] * sm[fe_route_nm[c0 + k] >> 4]);
+    // routing bound: K sum_k |G_k R^a F_m| <= sum_n b_n / |R|^(n+1) with
+    // b_n = K sum_{k: 2m - |a| = n} |G_k| c_k p^-(m + 1/2); rounded up to float
+    double b[FE_NCLASS], pm[FE_NCLASS];
+    pm[0] = 1.0 / sqrt(r[0]);
+    for (int m = 1; m <= L; ++m) pm[m] = pm[m - 1] / r[0];
+    for (int n = 0; n <= L; ++n) b[n] = 0.0;
+    for (int k = 0; k < NT; ++k) {
+      const unsigned nm = fe_route_nm[c0 + k];
+      b[nm & 15u] += fabs(r[6 + k]) * fe_route_c[c0 + k] * pm[nm >> 4];
+    }
+    for (int n = 0; n <= L; ++n) o[12 + 2 * NT + n] = __double2float_ru(r[4] * b[n]);
+    for (int k = 13 + 2 * NT + L; k < R32; ++k) o[k] = 0.0f;
   }
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) hdr->has32 = 1;
 }

@@ -3,11 +3,13 @@
 // FP32 for the per-pair Boys vector, the monomial/Horner polynomial and the
 // products; FP64 where FP32 would not hold the error budget:
 //
-//  * routing: for every pair and every point the bound K*bound/|R| (the
-//    reference's screening bound, fastesp/esp.py:251-254, evaluated at the
-//    point) bounds sum_k |G_k R^a F_m|; when it reaches ``tau`` for any point
-//    of a warp's point set (tested as |R|^2 <= (K*bound/tau)^2), that
-//    (pair, warp) is evaluated in FP64 instead.  fe_eval_f32_kernel takes the
+//  * routing: the FP32 rounding error of a pair's contribution scales with
+//    K sum_k |G_k R^a F_m(p R^2)|, which is at most sum_n b_n / |R|^(n+1)
+//    (F_m(T) <= Gamma(m + 1/2) / (2 T^(m + 1/2)), and |R^a| <= |R|^|a| times
+//    the maximum of |u^a| on the unit sphere; n = 2m - |a|, the b_n computed by
+//    the table build in FP64 and stored rounded up).  When that bound reaches
+//    ``tau`` for any point of a warp's point set, the (pair, warp) is
+//    evaluated in FP64 instead.  fe_eval_f32_kernel takes the
 //    decision, evaluates every (pair, warp) left in FP32 and records the others
 //    as one bit per (pair, warp) in a routing mask in the workspace;
 //    fe_eval_fix64_kernel evaluates exactly those in FP64 from the pairs' FP64
@@ -67,14 +69,17 @@ FE_DEV void fe_two_sum(float& hi, float& lo, float b) {
   lo += err;
 }
 
-// The routing test of one pair for this thread's points; identical in both
-// kernels (explicit fmaf, MUFU rsqrt), so their warp votes agree bit for bit.
-template <int NP>
+// The routing test of one class-L pair for this thread's points: the pair is
+// routed for the warp when the bound sum_n b_n / |R|^(n+1) (record floats
+// after the coefficients) reaches tau for any of the warp's points.  Written
+// !(bound < tau) so that a NaN or overflowing bound (a point on the pair's
+// centre) routes.
+template <int L, int NP>
 FE_DEV bool fe_route(const float* __restrict__ rec, const float (&cxh)[NP], const float (&cyh)[NP],
                      const float (&czh)[NP], const float (&cxl)[NP], const float (&cyl)[NP],
                      const float (&czl)[NP], float (&x)[NP], float (&y)[NP], float (&z)[NP],
                      float (&r2)[NP], float (&ir)[NP], float tau) {
-  const float kb = rec[10];
+  const float* bn = rec + 12 + 2 * fe_class_nterm[L];
   bool need = false;
 #pragma unroll
   for (int j = 0; j < NP; ++j) {
@@ -83,7 +88,10 @@ FE_DEV bool fe_route(const float* __restrict__ rec, const float (&cxh)[NP], cons
     z[j] = __fadd_rn(__fsub_rn(czh[j], rec[4]), __fsub_rn(czl[j], rec[7]));
     r2[j] = fmaf(x[j], x[j], fmaf(y[j], y[j], __fmul_rn(z[j], z[j])));
     ir[j] = rsqrtf(r2[j]);
-    need |= !(__fmul_rn(kb, ir[j]) < tau);
+    float bound = bn[L];
+#pragma unroll
+    for (int n = L - 1; n >= 0; --n) bound = fmaf(bound, ir[j], bn[n]);
+    need |= !(__fmul_rn(bound, ir[j]) < tau);
   }
   return __any_sync(0xffffffffu, need);
 }
@@ -118,7 +126,7 @@ FE_DEV void fe_tile_f32(const float* __restrict__ rec, int first, int n, int hi,
   for (int i = 0; i < n; ++i, rec += S32) {
     const int gi = first + i;
     float x[NP], y[NP], z[NP], r2[NP], ir[NP];
-    const bool routed = fe_route<NP>(rec, cxh, cyh, czh, cxl, cyl, czl, x, y, z, r2, ir, tau);
+    const bool routed = fe_route<L, NP>(rec, cxh, cyh, czh, cxl, cyl, czl, x, y, z, r2, ir, tau);
     bits |= unsigned(routed) << (gi & 31);
     if ((gi & 31) == 31 || gi + 1 == hi) {
       if (lane0 && mw) mw[gi >> 5] = bits;
@@ -154,16 +162,14 @@ FE_DEV void fe_two_sum2(float2& hi, float2& lo, float2 b) {
 #endif
 }
 
-template <int NQ>
+template <int L, int NQ>
 FE_DEV bool fe_route2(const float* __restrict__ rec, const float2 (&cxh)[NQ],
                       const float2 (&cyh)[NQ], const float2 (&czh)[NQ], const float2 (&cxl)[NQ],
                       const float2 (&cyl)[NQ], const float2 (&czl)[NQ], float2 (&x)[NQ],
                       float2 (&y)[NQ], float2 (&z)[NQ], float2 (&r2)[NQ], float2 (&ir)[NQ],
                       float tau) {
-  // K*bound/|R| >= tau  <=>  |R|^2 <= (K*bound/tau)^2 (also for K*bound = +inf);
-  // ``tau`` here is 1/tau
-  const float reach = __fmul_rn(rec[10], tau);
-  const float reach2 = __fmul_rn(reach, reach);
+  // fe_route for two points per lane: bound sum_n b_n / |R|^(n+1) in Horner form in 1/|R|
+  const float* bn = rec + 12 + 2 * fe_class_nterm[L];
   const float2 pxh = fe_f2(rec[2]), pyh = fe_f2(rec[3]), pzh = fe_f2(rec[4]);
   const float2 pxl = fe_f2(rec[5]), pyl = fe_f2(rec[6]), pzl = fe_f2(rec[7]);
   bool need = false;
@@ -174,7 +180,11 @@ FE_DEV bool fe_route2(const float* __restrict__ rec, const float2 (&cxh)[NQ],
     z[q] = (czh[q] - pzh) + (czl[q] - pzl);
     r2[q] = fe_fma(x[q], x[q], fe_fma(y[q], y[q], z[q] * z[q]));
     ir[q] = make_float2(rsqrtf(r2[q].x), rsqrtf(r2[q].y));
-    need |= (r2[q].x <= reach2) || (r2[q].y <= reach2);
+    float2 bound = fe_f2(bn[L]);
+#pragma unroll
+    for (int n = L - 1; n >= 0; --n) bound = fe_fma(bound, ir[q], fe_f2(bn[n]));
+    bound = bound * ir[q];
+    need |= !(bound.x < tau) || !(bound.y < tau);
   }
   return __any_sync(0xffffffffu, need);
 }
@@ -184,7 +194,7 @@ FE_DEV void fe_tile_f32x2(const float* __restrict__ rec, int first, int n, int h
                           const float2 (&cxh)[NQ], const float2 (&cyh)[NQ],
                           const float2 (&czh)[NQ], const float2 (&cxl)[NQ],
                           const float2 (&cyl)[NQ], const float2 (&czl)[NQ], float2 (&ahi)[NQ],
-                          float2 (&alo)[NQ], const float* __restrict__ grid, float inv_tau,
+                          float2 (&alo)[NQ], const float* __restrict__ grid, float tau,
                           unsigned* __restrict__ mw, unsigned& bits) {
   constexpr int S32 = fe_class_rec32[L];
   const bool lane0 = (threadIdx.x & 31) == 0;
@@ -192,7 +202,7 @@ FE_DEV void fe_tile_f32x2(const float* __restrict__ rec, int first, int n, int h
   for (int i = 0; i < n; ++i, rec += S32) {
     const int gi = first + i;
     float2 x[NQ], y[NQ], z[NQ], r2[NQ], ir[NQ];
-    const bool routed = fe_route2<NQ>(rec, cxh, cyh, czh, cxl, cyl, czl, x, y, z, r2, ir, inv_tau);
+    const bool routed = fe_route2<L, NQ>(rec, cxh, cyh, czh, cxl, cyl, czl, x, y, z, r2, ir, tau);
     bits |= unsigned(routed) << (gi & 31);
     if ((gi & 31) == 31 || gi + 1 == hi) {
       if (lane0 && mw) mw[gi >> 5] = bits;
@@ -292,7 +302,6 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
     fe_flag(FE_ST_OVERFLOW);
   }
   unsigned bits = 0u;
-  const float inv_tau = 1.0f / a.tau;
   for (int i = 0; i < total; ++i) {
     if (!pipe.wait(i)) {
       pipe.abort(i);
@@ -304,7 +313,7 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
     unsigned* mw = mrow ? mrow + w.woff[L] : nullptr;
     if constexpr (PACKED) {
 #define FE_CALL32(l) fe_tile_f32x2<l, NQ>(rec, first, n, w.hi[L], cxh2, cyh2, czh2, cxl2, cyl2, \
-                                          czl2, ahi2, alo2, grid, inv_tau, mw, bits)
+                                          czl2, ahi2, alo2, grid, a.tau, mw, bits)
       FE_MX_SWITCH(FE_CALL32)
 #undef FE_CALL32
     } else {

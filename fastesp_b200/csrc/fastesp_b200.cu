@@ -632,8 +632,11 @@ int eval_launch(const char* who, const void* d_table, const double* d_pts, int n
   return FE_OK;
 }
 
-// Default FP64 routing threshold of the mixed evaluator (a.u.).
-constexpr double kTauDefault = 0.1;
+// Default FP64 routing threshold of the mixed evaluator (a.u.): the largest
+// setting that kept the error against the FP64 path below 1e-6 a.u., with a
+// margin, on the 54-atom l<=3 system (three 30000-point surface samples and the
+// 568,950-point cubic grid, worst 7.7e-7; 0.05 reached 1.02e-6 on the grid).
+constexpr double kTauDefault = 0.04;
 
 }  // namespace
 

@@ -21,6 +21,7 @@ For every angular class L = la + lb (0..8) this emits
 """
 from __future__ import annotations
 
+import math
 import sys
 from functools import lru_cache
 from pathlib import Path
@@ -193,6 +194,29 @@ def consumption_order(L):
     """Term indices k in the order the class-L code reads them = record order."""
     build, _, _ = poly_variant(L)
     return build(L)[1].order()
+
+
+def route_constants(L):
+    """Routing-bound constants of the mixed path, per record position of class L.
+
+    Returns [(n, m, c)] with |G R^a F_m(p R^2)| <= |G| c p^-(m + 1/2) / |R|^(n + 1),
+    n = 2m - |a|: from F_m(T) <= Gamma(m + 1/2) / (2 T^(m + 1/2)) and
+    |R^a| <= |R|^|a| max_{|u|=1} |u^a|, the maximum of ux^ax uy^ay uz^az on the
+    unit sphere being sqrt(ax^ax ay^ay az^az / |a|^|a|) (at u_i^2 = a_i / |a|).
+    """
+    keys, _ = H.class_terms(L)
+    out = []
+    for k in consumption_order(L):
+        ax, ay, az, m = keys[k]
+        deg = ax + ay + az
+        num = 1.0
+        for v in (ax, ay, az):
+            num *= float(v) ** v if v else 1.0
+        mf = (num / float(deg) ** deg) ** 0.5 if deg else 1.0
+        n = 2 * m - deg
+        assert 0 <= n <= L and m < 16
+        out.append((n, m, math.gamma(m + 0.5) / 2.0 * mf))
+    return out
 
 
 def poly_functions(L):
@@ -369,13 +393,38 @@ def boys_grid32():
             for i in range(nrow)]
 
 
+def boys_scale(m):
+    """s_m = (sqrt(pi)/2) (2m-1)!!/2^m, the large-T limit of F_m(T) T^(m+1/2).
+
+    The packed FP32 evaluator works with F^_m = F_m / s_m: its asymptotic form
+    is T^-(m+1/2) and its recursions have exactly representable constants, so
+    no FP32 rounding of a constant biases every pair alike; the table build
+    folds s_m into the FP32 coefficients in FP64."""
+    import mpmath as mp
+    mp.mp.dps = 30
+    s = mp.sqrt(mp.pi) / 2
+    for j in range(1, m + 1):
+        s *= mp.mpf(2 * j - 1) / 2
+    return s
+
+
 def boys_grid32_scaled(M):
-    """Rows F_(M+k)(i h)/k!, k < TAYLOR_K32, of the FP32 grid (30 digits)."""
+    """Rows F_(M+k)(i h)/(k! s_M), k < TAYLOR_K32, of the FP32 grid (30 digits):
+    the Taylor polynomial of F^_M = F_M / s_M in d directly."""
     import mpmath as mp
     mp.mp.dps = 30
     nrow = int(round(GRID_TMAX32 / GRID_H32)) + 2
-    return [[float(boys_mp(M + k, mp.mpf(i) * mp.mpf(GRID_H32)) / mp.factorial(k))
+    sM = boys_scale(M)
+    return [[float(boys_mp(M + k, mp.mpf(i) * mp.mpf(GRID_H32)) / (mp.factorial(k) * sM))
              for k in range(TAYLOR_K32)] for i in range(nrow)]
+
+
+def split_f32(v):
+    """(hi, lo) floats with hi + lo = v to about 48 bits."""
+    import numpy as np
+    hi = float(np.float32(float(v)))
+    lo = float(np.float32(float(v - hi)))
+    return hi, lo
 
 
 def asym_thresholds(rel=1e-16):
@@ -455,7 +504,14 @@ def main() -> int:
     # per-order scaled FP32 rows for the packed evaluator: F_(M+k)(i h) / k!
     ms = 6
     out.append(f"#define FE_BOYS32S_MMAX {ms}")
-    out.append("// F_(M+k)(i h)/k!, M = 0..FE_BOYS32S_MMAX, k < FE_BOYS32_TAYLOR_K: row (M, i) at")
+    # kappa_m = 1 / (2 s_m) and 1 / s_m as float hi/lo pairs (FP32 Boys recursions)
+    kap = [split_f32(1 / (2 * boys_scale(m))) for m in range(MMAX + 1)]
+    sinv = [split_f32(1 / boys_scale(m)) for m in range(MMAX + 1)]
+    for name, vals, k in (("fe_boys32_kappa_hi", kap, 0), ("fe_boys32_kappa_lo", kap, 1),
+                          ("fe_boys32_sinv_hi", sinv, 0), ("fe_boys32_sinv_lo", sinv, 1)):
+        out.append(f"static constexpr float {name}[FE_MMAX + 1] = {{"
+                   + ", ".join(repr(v[k]) + "f" for v in vals) + "};")
+    out.append("// F_(M+k)(i h)/(k! s_M), M = 0..FE_BOYS32S_MMAX, k < FE_BOYS32_TAYLOR_K: row (M, i) at")
     out.append("// (M * FE_BOYS32_NROW + i) * FE_BOYS32_TAYLOR_K (Taylor polynomial in d directly)")
     out.append("__device__ const float fe_boys_grid32s[(FE_BOYS32S_MMAX + 1) * FE_BOYS32_NROW"
                " * FE_BOYS32_TAYLOR_K] = {")
@@ -503,6 +559,19 @@ def main() -> int:
         pos = {k: i for i, k in enumerate(consumption_order(L))}
         out.append(f"__constant__ short fe_gpos_L{L}[{H.n_terms(L)}] = {{"
                    + ", ".join(str(pos[k]) for k in range(H.n_terms(L))) + "};")
+    out.append("")
+    offs, cs, nms = [], [], []
+    for L in range(LMAX + 1):
+        offs.append(len(cs))
+        for n, m, c in route_constants(L):
+            cs.append(c)
+            nms.append(n | (m << 4))
+    out.append("// mixed-path routing bound: record position j of class L has constant")
+    out.append("// fe_route_c[fe_route_off[L] + j] and n | m << 4 in fe_route_nm (n = 2m - |a|)")
+    out.append("__constant__ int fe_route_off[FE_NCLASS] = {" + ", ".join(map(str, offs)) + "};")
+    out.append(f"__constant__ double fe_route_c[{len(cs)}] = {{" + ", ".join(repr(c) for c in cs) + "};")
+    out.append(f"__constant__ unsigned char fe_route_nm[{len(nms)}] = {{"
+               + ", ".join(map(str, nms)) + "};")
     out.append("")
     out.append("static constexpr int fe_class_polyops[FE_NCLASS] = {"
                + ", ".join(map(str, nops)) + "};")

@@ -20,8 +20,9 @@
 // a 16-byte load yields two coefficients each already a {g, g} operand pair
 // of the packed FP32x2 arithmetic:
 // [p_hi, p_lo, Px_hi, Py_hi, Pz_hi, Px_lo, Py_lo, Pz_lo, K_hi, K_lo, K*bound,
-//  p^-1/2, G_0, G_0, G_1, G_1, ..., G_(nt-1), G_(nt-1), pad to 16 bytes]
-// (G in the same consumption order as the FP64 record).
+//  p^-1/2, G_0, G_0, G_1, G_1, ..., G_(nt-1), G_(nt-1), b_0, .., b_L, pad to
+//  16 bytes] (G in the same consumption order as the FP64 record; b_n the
+// coefficients of the routing bound sum_n b_n / |R|^(n+1), eval_mixed.cuh).
 //
 // The source section maps every record of a table built on the device back to
 // the builder's work item (shell pair and primitive indices), so the adjoint

@@ -146,8 +146,9 @@ int fe_esp_fp64(const void* d_table, const double* d_pts, int n_pts, double* d_o
 
 /* Mixed precision: the Boys vector, monomials and term products in FP32 with a
  * compensated (two-sum) FP32 accumulation per point; a pair is evaluated in
- * FP64 for a warp of points whenever its bound K*bound/|R| reaches ``tau``
- * (a.u.; <= 0 selects the default 0.1) for one of them; the split sums, the
+ * FP64 for a warp of points whenever the bound sum_n b_n/|R|^(n+1) on
+ * K sum_k |G_k R^alpha F_m| (b_n formed by the table build from G, p and K)
+ * reaches ``tau`` (a.u.; <= 0 selects the default) for one of them; the split sums, the
  * nuclear term and the final subtraction are FP64.  Same result as
  * fe_esp_fp64 within 1e-6 a.u. on the tested systems.  ``d_n64`` (nullable)
  * accumulates the number of (pair, warp) evaluations routed to FP64.  No

@@ -320,13 +320,19 @@ def test_mixed_routing_extremes(tz6_system):
     assert np.abs(none64 - v64).max() < 1e-3
 
 
-def test_mixed_imported_table_is_all_fp64(tmp_path, small_system):
-    """pairs.bin carries no screening bound, so the mixed path evaluates in FP64."""
+def test_mixed_imported_table_routes_like_built(tmp_path, small_system):
+    """pairs.bin carries no screening bound, but the routing bound of the mixed
+    path comes from each pair's G, p and K alone: an imported table routes and
+    evaluates exactly as the table it was written from."""
     wfn, basis, P, g = small_system
     tab = build_table(wfn, basis, g["density"], g["points"], tol=1e-12)
     tab.write(tmp_path / "pairs.bin")
     back = PairTable.read(tmp_path / "pairs.bin")
-    np.testing.assert_allclose(back.esp(precision="mixed"), g["esp_t12"], rtol=0, atol=1e-11)
+    vm, n_built = tab.esp_stats()
+    vb, n_back = back.esp_stats()
+    assert n_back == n_built
+    np.testing.assert_array_equal(vb, vm)
+    assert np.abs(vb - g["esp_t12"]).max() <= MIXED_TOL
 
 
 @pytest.mark.parametrize("npts", [300, 30000])

@@ -179,7 +179,51 @@ def test_record_strides_are_16_byte_multiples():
     for L in range(9):
         nt = H.n_terms(L)
         assert H.record_stride(L) * 8 % 16 == 0 and H.record_stride(L) >= 6 + nt
-        assert H.record_stride_f32(L) * 4 % 16 == 0 and H.record_stride_f32(L) >= 12 + 2 * nt
+        assert H.record_stride_f32(L) * 4 % 16 == 0 and H.record_stride_f32(L) >= 12 + 2 * nt + L + 1
+
+
+def _gen_module():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "gen_classes", Path(__file__).resolve().parents[1] / "fastesp_b200" / "csrc" / "gen_classes.py")
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    return gen
+
+
+def test_mixed_routing_bound_holds(tz6_system):
+    """The mixed path's routing bound sum_n b_n / |R|^(n+1) (constants from the
+    generator, b_n as the table build forms them) is never below the exact
+    K sum_k |G_k R^a F_m(p R^2)| of a pair, near or far, on every class."""
+    import oracle.esp_oracle as O
+    gen = _gen_module()
+    wfn, basis, P, g = tz6_system
+    pp = O.primitive_pairs(wfn.shells, wfn.coords, g["density"])
+    rng = np.random.default_rng(3)
+    pts = np.asarray(g["points"], float)
+    worst = 0.0
+    for L in sorted(set(int(v) for v in pp["L"])):
+        keys, _ = H.class_terms(L)
+        _, _, _, mono, mvals, _ = O.pair_type(L)
+        assert [tuple(k) for k in keys] == [(*map(int, a), int(m)) for a, m in zip(mono, mvals)]
+        rc = gen.route_constants(L)
+        order = gen.consumption_order(L)
+        idx = np.nonzero(pp["L"] == L)[0]
+        for i in rng.choice(idx, min(len(idx), 200), replace=False):
+            p, K, G = pp["p"][i], pp["K"][i], np.asarray(pp["G"][i])
+            b = np.zeros(L + 1)
+            for j, k in enumerate(order):
+                n, m, c = rc[j]
+                b[n] += abs(G[k]) * c * p ** -(m + 0.5)
+            b *= K
+            for s in (1.0, 0.3, 0.05):
+                R = (pts[rng.integers(len(pts))] - pp["P"][i]) * s
+                r = float(np.linalg.norm(R))
+                F = [O.boys(int(m), np.array([p * r * r]))[0] for m in mvals]
+                exact = K * np.sum(np.abs(G) * np.abs(np.prod(R[None, :] ** mono, 1)) * F)
+                bound = np.sum(b * r ** -(np.arange(L + 1) + 1.0))
+                worst = max(worst, exact / bound)
+    assert 0.0 < worst <= 1.0 + 1e-12, worst
 
 
 def test_molden_reader_fast_and_fallback_paths_agree(tmp_path):
