@@ -219,7 +219,7 @@ FE_DEV void fe_tile_f32x2(const float* __restrict__ rec, int first, int n, int h
   }
 }
 
-// FP64 evaluation of one routed pair (record ``rec64`` in shared memory) for
+// FP64 evaluation of one routed pair (its FP64 record ``rec64``) for
 // this thread's points, two at a time for instruction-level parallelism.
 template <int L, int NP>
 FE_DEV void fe_pair_fix64(const double* __restrict__ rec64, const double (&cx)[NP],
@@ -342,21 +342,16 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
 
 // The FP64 part: grid row y takes one class and a part of its mask words
 // (fe_class_rows, class-major so that concurrently running blocks execute the
-// same class's code).  The block walks its four warps' mask rows 32 words at a
-// time; for every word it takes the union of the warps' bits, copies the FP64
-// records of those pairs into shared memory in batches (all 128 threads), and
-// each warp then evaluates, for its points, the batch's pairs whose bit is set
-// in its own row.  Routed pairs are mostly routed for every warp, so a record
-// is fetched once per block instead of once per warp.  Every warp accumulates
-// its pairs in pair order and every grid row writes its own partial sums, so
-// the result is deterministic.
-#define FE_FIX_BUF 2304     // doubles of the record batch (16 class-6 records)
-
+// same class's code).  Each warp walks its own mask row, 32 words at a time
+// (one word per lane, the non-empty ones found by a ballot), and evaluates
+// every pair whose bit is set for its points, reading the pair's FP64 record
+// with warp-uniform loads (L1/L2: the warps of a block that route the same pair
+// read it at about the same time).  No block barrier: a warp with nothing
+// routed finishes early.  Every warp accumulates its pairs in pair order and
+// every grid row writes its own partial sums, so the result is deterministic.
 template <int MINB, int LLO, int LHI>
 __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_fix64_kernel(const FeMixedArgs a) {
   constexpr int NP = FE_MX_NP, NT = FE_MX_NT, NW = FE_MX_NT / 32;
-  __shared__ __align__(16) double buf[FE_FIX_BUF];
-  __shared__ unsigned wb[NW][32];
   __shared__ FeBlockWork w;
   const FeTableHdr* hdr = reinterpret_cast<const FeTableHdr*>(a.table);
   const int tid = threadIdx.x, lane = tid & 31, wi = tid >> 5;
@@ -388,49 +383,24 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_fix64_kernel(const FeM
     const int w0 = int((long long)nw * part / nparts);
     const int w1 = int((long long)nw * (part + 1) / nparts);
     const int S64 = fe_c_rec64[L];
-    const int B = min(32, FE_FIX_BUF / S64);          // records per batch
     const double* base = reinterpret_cast<const double*>(a.table + hdr->off64[L]);
     const unsigned* mrow = a.mask + (warp0 + wi) * w.wtotal + w.woff[L];
     for (int c0 = w0; c0 < w1; c0 += 32) {
-      __syncthreads();                                // wb and buf free
-      wb[wi][lane] = c0 + lane < w1 ? mrow[c0 + lane] : 0u;
-      __syncthreads();
-      const int kn = min(32, w1 - c0);
-      for (int k = 0; k < kn; ++k) {
-        unsigned rem = 0u;
-#pragma unroll
-        for (int v = 0; v < NW; ++v) rem |= wb[v][k];
-        const unsigned mine = wb[wi][k];
+      const unsigned wv = c0 + lane < w1 ? mrow[c0 + lane] : 0u;
+      unsigned nz = __ballot_sync(0xffffffffu, wv != 0u);
+      while (nz) {                                    // warp-uniform
+        const int k = __ffs(nz) - 1;
+        nz &= nz - 1;
+        unsigned mine = __shfl_sync(0xffffffffu, wv, k);
         const size_t pair0 = size_t(c0 + k) * 32;
-        while (rem) {                                 // block-uniform
-          // the next batch: the lowest B set bits of rem
-          unsigned bm = 0u, r = rem;
-          for (int t = 0; t < B && r; ++t) {
-            bm |= r & (0u - r);
-            r &= r - 1;
-          }
-          rem = r;
-          const int nb = __popc(bm);
-          // copy: record t of the batch (its t-th set bit) by warp t % NW
-          for (int t = wi; t < nb; t += NW) {
-            unsigned r2 = bm;                         // its t-th set bit
-            for (int u = 0; u < t; ++u) r2 &= r2 - 1;
-            const int bit = __ffs(r2) - 1;
-            const double* src = base + (pair0 + bit) * S64;
-            for (int q = lane; q < S64; q += 32) buf[t * S64 + q] = __ldg(src + q);
-          }
-          __syncthreads();
-          unsigned todo = bm & mine;
-          while (todo) {                              // warp-uniform
-            const int bit = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const int t = __popc(bm & ((1u << bit) - 1u));
-            ++n64;
-#define FE_CALLP(l) fe_pair_fix64<l, NP>(buf + t * S64, cx, cy, cz, a64)
-            FE_MX_SWITCH(FE_CALLP)
+        while (mine) {
+          const int bit = __ffs(mine) - 1;
+          mine &= mine - 1;
+          ++n64;
+          const double* rec = base + (pair0 + bit) * S64;
+#define FE_CALLP(l) fe_pair_fix64<l, NP>(rec, cx, cy, cz, a64)
+          FE_MX_SWITCH(FE_CALLP)
 #undef FE_CALLP
-          }
-          __syncthreads();                            // buf free for the next batch
         }
       }
     }
