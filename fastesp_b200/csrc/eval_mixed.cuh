@@ -21,10 +21,11 @@
 //    g-shell classes run scalar.
 //  * R = C - P from float hi/lo splits of both coordinates, so R carries about
 //    one float ulp of R itself rather than of |C|.
-//  * accumulation: FP32 contributions into a compensated two-sum pair per
-//    point (TwoSum: Knuth, The Art of Computer Programming vol. 2, 4.2.2), FP64
-//    contributions into an FP64 sum; the splits, the nuclear term and the final
-//    nuclear - electron subtraction are FP64.
+//  * accumulation: every pair's FP32 contribution K s, rounded once, is added
+//    to an FP64 sum per point (the FP64 pipe is otherwise idle in the FP32
+//    kernel, so two conversions and two DADDs per point pair cost less than a
+//    compensated FP32 two-sum); FP64 contributions into an FP64 sum; the splits,
+//    the nuclear term and the final nuclear - electron subtraction are FP64.
 //
 // Grid and pipeline of the FP32 kernel as eval_f64 (class-major grid rows,
 // points in registers, record tiles streamed to shared memory by 1-D TMA bulk
@@ -60,14 +61,6 @@ __constant__ int fe_c_tile32[FE_NCLASS] = {
   FE_STAGE_BYTES / (4 * fe_class_rec32[4]), FE_STAGE_BYTES / (4 * fe_class_rec32[5]),
   FE_STAGE_BYTES / (4 * fe_class_rec32[6]), FE_STAGE_BYTES / (4 * fe_class_rec32[7]),
   FE_STAGE_BYTES / (4 * fe_class_rec32[8])};
-
-FE_DEV void fe_two_sum(float& hi, float& lo, float b) {
-  const float s = hi + b;
-  const float bb = s - hi;
-  const float err = (hi - (s - bb)) + (b - bb);
-  hi = s;
-  lo += err;
-}
 
 // The routing test of one class-L pair for this thread's points: the pair is
 // routed for the warp when the bound sum_n b_n / |R|^(n+1) (record floats
@@ -118,8 +111,8 @@ template <int L, int NP>
 FE_DEV void fe_tile_f32(const float* __restrict__ rec, int first, int n, int hi,
                         const float (&cxh)[NP], const float (&cyh)[NP], const float (&czh)[NP],
                         const float (&cxl)[NP], const float (&cyl)[NP], const float (&czl)[NP],
-                        float (&ahi)[NP], float (&alo)[NP], const float* __restrict__ grid,
-                        float tau, unsigned* __restrict__ mw, unsigned& bits) {
+                        double (&acc)[NP], const float* __restrict__ grid, float tau,
+                        unsigned* __restrict__ mw, unsigned& bits) {
   constexpr int S32 = fe_class_rec32[L];
   const bool lane0 = (threadIdx.x & 31) == 0;
 #pragma unroll 1
@@ -139,29 +132,14 @@ FE_DEV void fe_tile_f32(const float* __restrict__ rec, int first, int n, int hi,
     for (int j = 0; j < NP; ++j) fe_boys_f32<L>(pe * r2[j], ir[j] * rsp, grid, F[j]);
     fe_poly<L, float, NP>(rec + 12, x, y, z, F, s);
 #pragma unroll
-    for (int j = 0; j < NP; ++j) fe_two_sum(ahi[j], alo[j], K * s[j]);
+    for (int j = 0; j < NP; ++j) acc[j] += double(K * s[j]);
   }
 }
 
 // The same routing test and FP32 evaluation with two points per float2 lane
 // (packed FP32x2 instructions; point 2q + e of the thread in lane e of q).
-// Lane by lane the operations are those of fe_route / fe_tile_f32, so the
-// results are the same bit for bit.
-FE_DEV void fe_two_sum2(float2& hi, float2& lo, float2 b) {
-#ifdef FE_FAST2SUM
-  const float2 s = hi + b;
-  const float2 err = b - (s - hi);
-  hi = s;
-  lo = lo + err;
-#else
-  const float2 s = hi + b;
-  const float2 bb = s - hi;
-  const float2 err = (hi - (s - bb)) + (b - bb);
-  hi = s;
-  lo = lo + err;
-#endif
-}
-
+// Lane by lane the routing test is that of fe_route; the Boys vector comes
+// from the per-order scaled rows (fe_boys_f32x2).
 template <int L, int NQ>
 FE_DEV bool fe_route2(const float* __restrict__ rec, const float2 (&cxh)[NQ],
                       const float2 (&cyh)[NQ], const float2 (&czh)[NQ], const float2 (&cxl)[NQ],
@@ -193,8 +171,8 @@ template <int L, int NQ>
 FE_DEV void fe_tile_f32x2(const float* __restrict__ rec, int first, int n, int hi,
                           const float2 (&cxh)[NQ], const float2 (&cyh)[NQ],
                           const float2 (&czh)[NQ], const float2 (&cxl)[NQ],
-                          const float2 (&cyl)[NQ], const float2 (&czl)[NQ], float2 (&ahi)[NQ],
-                          float2 (&alo)[NQ], const float* __restrict__ grid, float tau,
+                          const float2 (&cyl)[NQ], const float2 (&czl)[NQ],
+                          double (&acc)[2 * NQ], const float* __restrict__ grid, float tau,
                           unsigned* __restrict__ mw, unsigned& bits) {
   constexpr int S32 = fe_class_rec32[L];
   const bool lane0 = (threadIdx.x & 31) == 0;
@@ -215,7 +193,11 @@ FE_DEV void fe_tile_f32x2(const float* __restrict__ rec, int first, int n, int h
     for (int q = 0; q < NQ; ++q) fe_boys_f32x2<L>(pe * r2[q], ir[q] * rsp, grid, F[q]);
     fe_poly32x2<L, NQ>(rec + 12, x, y, z, F, s);
 #pragma unroll
-    for (int q = 0; q < NQ; ++q) fe_two_sum2(ahi[q], alo[q], K * s[q]);
+    for (int q = 0; q < NQ; ++q) {
+      const float2 v = K * s[q];
+      acc[2 * q] += double(v.x);
+      acc[2 * q + 1] += double(v.y);
+    }
   }
 }
 
@@ -273,12 +255,13 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
   const FeTableHdr* hdr = reinterpret_cast<const FeTableHdr*>(a.table);
   const int tid = threadIdx.x;
   for (int k = tid; k < GRIDN; k += NT) grid[k] = PACKED ? fe_boys_grid32s[k] : fe_boys_grid32[k];
-  float cxh[NP], cyh[NP], czh[NP], cxl[NP], cyl[NP], czl[NP], ahi[NP], alo[NP];
+  float cxh[NP], cyh[NP], czh[NP], cxl[NP], cyl[NP], czl[NP];
+  double acc[NP];
   const int p0 = int(blockIdx.x) * (NT * NP) + tid;
   fe_load_points_split<NP>(a.pts, a.npts, p0, NT, cxh, cyh, czh, cxl, cyl, czl);
 #pragma unroll
-  for (int j = 0; j < NP; ++j) ahi[j] = alo[j] = 0.0f;
-  float2 cxh2[NQ], cyh2[NQ], czh2[NQ], cxl2[NQ], cyl2[NQ], czl2[NQ], ahi2[NQ], alo2[NQ];
+  for (int j = 0; j < NP; ++j) acc[j] = 0.0;
+  float2 cxh2[NQ], cyh2[NQ], czh2[NQ], cxl2[NQ], cyl2[NQ], czl2[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
     cxh2[q] = make_float2(cxh[2 * q], cxh[2 * q + 1]);
@@ -287,7 +270,6 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
     cxl2[q] = make_float2(cxl[2 * q], cxl[2 * q + 1]);
     cyl2[q] = make_float2(cyl[2 * q], cyl[2 * q + 1]);
     czl2[q] = make_float2(czl[2 * q], czl[2 * q + 1]);
-    ahi2[q] = alo2[q] = make_float2(0.0f, 0.0f);
   }
   FeTilePipe pipe{a.table, fe_c_tile32, fe_c_rec32, hdr->off32, 4, fe_smem, full_bar, &w};
   int Lrow, part, nparts;
@@ -313,30 +295,21 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
     unsigned* mw = mrow ? mrow + w.woff[L] : nullptr;
     if constexpr (PACKED) {
 #define FE_CALL32(l) fe_tile_f32x2<l, NQ>(rec, first, n, w.hi[L], cxh2, cyh2, czh2, cxl2, cyl2, \
-                                          czl2, ahi2, alo2, grid, a.tau, mw, bits)
+                                          czl2, acc, grid, a.tau, mw, bits)
       FE_MX_SWITCH(FE_CALL32)
 #undef FE_CALL32
     } else {
 #define FE_CALL32(l) fe_tile_f32<l, NP>(rec, first, n, w.hi[L], cxh, cyh, czh, cxl, cyl, czl, \
-                                        ahi, alo, grid, a.tau, mw, bits)
+                                        acc, grid, a.tau, mw, bits)
       FE_MX_SWITCH(FE_CALL32)
 #undef FE_CALL32
     }
     pipe.release(i);
   }
-  if constexpr (PACKED) {
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) {
-      ahi[2 * q] = ahi2[q].x;
-      ahi[2 * q + 1] = ahi2[q].y;
-      alo[2 * q] = alo2[q].x;
-      alo[2 * q + 1] = alo2[q].y;
-    }
-  }
 #pragma unroll
   for (int j = 0; j < NP; ++j) {
     const int p = p0 + j * NT;
-    if (p < a.npts) a.partial[size_t(blockIdx.y) * a.ld + p] = double(ahi[j]) + double(alo[j]);
+    if (p < a.npts) a.partial[size_t(blockIdx.y) * a.ld + p] = acc[j];
   }
 }
 
