@@ -144,8 +144,8 @@ size_t fe_eval_ws_bytes_mixed(int n_pts, const int* cap);
 int fe_esp_fp64(const void* d_table, const double* d_pts, int n_pts, double* d_out,
                 void* d_ws, size_t ws_bytes, cudaStream_t stream);
 
-/* Mixed precision: the Boys vector, monomials and term products in FP32 with a
- * compensated (two-sum) FP32 accumulation per point; a pair is evaluated in
+/* Mixed precision: the Boys vector, monomials and term products in FP32, each
+ * pair's contribution accumulated in FP64 per point; a pair is evaluated in
  * FP64 for a warp of points whenever the bound sum_n b_n/|R|^(n+1) on
  * K sum_k |G_k R^alpha F_m| (b_n formed by the table build from G, p and K)
  * reaches ``tau`` (a.u.; <= 0 selects the default) for one of them; the split sums, the
