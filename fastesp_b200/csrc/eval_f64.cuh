@@ -25,7 +25,7 @@
 #define FE_STAGE_BYTES 16384
 #endif
 #ifndef FE_NSTAGE
-#define FE_NSTAGE 3
+#define FE_NSTAGE 2          // 2 stages leave more of the SM's shared/L1 to the L1 cache
 #endif
 
 struct FeEvalArgs {

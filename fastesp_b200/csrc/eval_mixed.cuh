@@ -248,8 +248,9 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
   extern __shared__ __align__(128) unsigned char fe_smem[];
   __shared__ uint64_t full_bar[FE_NSTAGE];
   __shared__ FeBlockWork w;
-  // packed classes: the per-order scaled rows; g-shell classes: the plain rows
-  constexpr int GRIDN = PACKED ? (FE_BOYS32S_MMAX + 1) * FE_BOYS32_NROW * FE_BOYS32_TAYLOR_K
+  // packed classes: the per-order scaled rows of orders 0..LHI (the highest
+  // order a class of the range asks for); g-shell classes: the plain rows
+  constexpr int GRIDN = PACKED ? (LHI + 1) * FE_BOYS32_NROW * FE_BOYS32_TAYLOR_K
                                : FE_BOYS32_NROW * FE_BOYS32_NTAB;
   __shared__ float grid[GRIDN];
   const FeTableHdr* hdr = reinterpret_cast<const FeTableHdr*>(a.table);

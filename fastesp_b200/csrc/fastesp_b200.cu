@@ -74,21 +74,28 @@ int sm_count() {
 #ifndef FE_MINB32
 #define FE_MINB32 3
 #endif
+#ifndef FE_MINB32LO
+#define FE_MINB32LO 4
+#endif
 #ifndef FE_MINBFIX
 #define FE_MINBFIX 4
 #endif
 constexpr int kEvalThreads = 128;
 constexpr int kNP64 = FE_NP64, kMinB64 = FE_MINB64;
-constexpr int kNP32 = FE_MX_NP, kMinB32 = FE_MINB32, kMinBFix = FE_MINBFIX;
+constexpr int kNP32 = FE_MX_NP, kMinB32 = FE_MINB32, kMinB32Lo = FE_MINB32LO, kMinBFix = FE_MINBFIX;
 
 // Class ranges of the two kernel instances of every evaluator: classes up to
 // FE_LSPLIT (s..f shell pairs) and the g-shell classes above it, compiled
 // separately so the common classes do not carry the registers of the largest.
 #define FE_LSPLIT 6
+// The packed FP32 kernel is split once more, at FE_MXSPLIT: classes 0..4 fit in
+// 128 registers and, with a 2-stage ring and their 5 Boys-grid orders in shared
+// memory, run 4 blocks per SM; classes 5..6 need 159 registers (3 per SM).
+#define FE_MXSPLIT 4
 
 struct EvalGeom {
   int nblk_x, ld;
-  int split[4];        // splits of: main, high (, FP64 part main, FP64 part high)
+  int split[5];        // FP64: main, high; mixed: FP32 0..4, 5..6, high, FP64 part main, high
   int nkern;
   size_t ws_rows() const {
     size_t r = 0;
@@ -115,11 +122,13 @@ EvalGeom eval_geom(int npts, int mode) {
   // every kernel needs at least one grid row per class of its range (fe_class_rows)
   const int nlo = FE_LSPLIT + 1, nhi = FE_NCLASS - 1 - FE_LSPLIT;
   if (mode == 1) {
-    g.nkern = 4;
-    g.split[0] = std::max(nlo, splits(kMinB32));
-    g.split[1] = std::max(nhi, hi_splits);
-    g.split[2] = std::max(nlo, splits(kMinBFix));
-    g.split[3] = std::max(nhi, hi_splits);
+    // classes 5..6 carry about an eighth of the FP32 work: two waves of their own
+    g.nkern = 5;
+    g.split[0] = std::max(FE_MXSPLIT + 1, splits(kMinB32Lo));
+    g.split[1] = std::max(FE_LSPLIT - FE_MXSPLIT, splits(kMinB32) / 4);
+    g.split[2] = std::max(nhi, hi_splits);
+    g.split[3] = std::max(nlo, splits(kMinBFix));
+    g.split[4] = std::max(nhi, hi_splits);
   } else {
     g.nkern = 2;
     g.split[0] = std::max(nlo, splits(kMinB64));
@@ -611,15 +620,17 @@ int eval_launch(const char* who, const void* d_table, const double* d_pts, int n
     a.n64 = d_n64;
     a.mask = reinterpret_cast<unsigned*>(static_cast<unsigned char*>(d_ws) + rows_bytes);
     a.mask_words = static_cast<long long>((ws_bytes - rows_bytes) / 4);
-    auto f0 = fe_eval_f32_kernel<kMinB32, 0, FE_LSPLIT>;
+    auto f0 = fe_eval_f32_kernel<kMinB32Lo, 0, FE_MXSPLIT>;
+    auto f0b = fe_eval_f32_kernel<kMinB32, FE_MXSPLIT + 1, FE_LSPLIT>;
     auto f1 = fe_eval_f32_kernel<1, FE_LSPLIT + 1, FE_NCLASS - 1>;
     auto x0 = fe_eval_fix64_kernel<kMinBFix, 0, FE_LSPLIT>;
     auto x1 = fe_eval_fix64_kernel<1, FE_LSPLIT + 1, FE_NCLASS - 1>;
-    const void* ks[4] = {(const void*)f0, (const void*)f1, (const void*)x0, (const void*)x1};
-    for (int k = 0; k < 4; ++k) {
+    const void* ks[5] = {(const void*)f0, (const void*)f0b, (const void*)f1, (const void*)x0,
+                         (const void*)x1};
+    for (int k = 0; k < 5; ++k) {
       a.nsplit = g.split[k];
       a.partial = next_rows(k);
-      const int dyn = k < 2 ? smem : 0;      // the FP64 part uses static buffers only
+      const int dyn = k < 3 ? smem : 0;      // the FP64 part uses static buffers only
       if (dyn) FE_CUDA(cudaFuncSetAttribute(ks[k], cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
       void* args[] = {&a};
       FE_CUDA(cudaLaunchKernel(ks[k], dim3(g.nblk_x, g.split[k]), dim3(FE_MX_NT), args, dyn, st));
