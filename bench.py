@@ -105,24 +105,73 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def peak_flops(torch, fp64=True):
+def peak_flops(torch, kind):
+    """Measured FMA throughput (FLOP/s) of this GPU: kind 0 scalar FP32, 1 FP64,
+    2 packed FP32x2 (fe_peak_run: 8 independent FMA chains per thread)."""
     from fastesp_b200 import _lib
     dev = torch.cuda.current_device()
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     blocks = sms * 8
     out = torch.empty(blocks, dtype=torch.float64, device="cuda")
-    iters = 1 << 14 if fp64 else 1 << 15
+    iters = 1 << 14 if kind == 1 else 1 << 15
+    per_iter = 32.0 if kind == 2 else 16.0
     for _ in range(2):
-        _lib.check(_lib.lib().fe_peak_run(int(fp64), iters, blocks, _lib.ptr(out), _lib.stream_ptr()))
+        _lib.check(_lib.lib().fe_peak_run(kind, iters, blocks, _lib.ptr(out), _lib.stream_ptr()))
     best = 0.0
     for _ in range(5):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        _lib.check(_lib.lib().fe_peak_run(int(fp64), iters, blocks, _lib.ptr(out), _lib.stream_ptr()))
+        _lib.check(_lib.lib().fe_peak_run(kind, iters, blocks, _lib.ptr(out), _lib.stream_ptr()))
         b.record()
         b.synchronize()
-        best = max(best, 16.0 * iters * 256 * blocks / (a.elapsed_time(b) * 1e-3))
+        best = max(best, per_iter * iters * 256 * blocks / (a.elapsed_time(b) * 1e-3))
     return best
+
+
+def build_flops(wfn):
+    """Algorithmic FLOPs of one table build without the point screen: every
+    primitive pair of every shell pair si <= sj (hermite.build_flops)."""
+    from fastesp_b200 import hermite as H
+    sh = wfn.shells
+    tot = 0
+    for i in range(len(sh)):
+        for j in range(i, len(sh)):
+            la, lb = sh[i].l, sh[j].l
+            tot += len(sh[i].exps) * len(sh[j].exps) * H.build_flops(min(la, lb), max(la, lb))
+    return float(tot)
+
+
+def build_pairs_count(wfn):
+    sh = wfn.shells
+    n = [len(s.exps) for s in sh]
+    return int(sum(n[i] * n[j] for i in range(len(sh)) for j in range(i, len(sh))))
+
+
+def per_class_rates(torch, tab, pts_d, npts, flush, peak64, peak32, reps=5):
+    """Time each class alone (fe_electron_classes) in both precisions: ms,
+    algorithmic TFLOP/s and the fraction of the FP64 / FP32 peak."""
+    from fastesp_b200 import _lib, hermite as H
+    L_ = _lib.lib()
+    out = torch.empty(npts, dtype=torch.float64, device=pts_d.device)
+    ws = torch.empty(max(tab.ws_bytes(npts, "fp64"), tab.ws_bytes(npts, "mixed")),
+                     dtype=torch.uint8, device=pts_d.device)
+    rows = []
+    for L, c in enumerate(tab.counts):
+        if not c:
+            continue
+        fl = float(c) * H.eval_flops(L) * npts
+        row = {"class": L, "pairs": int(c), "flops": fl}
+        for prec, name, peak in ((0, "fp64", peak64), (1, "mixed", peak32)):
+            def run():
+                _lib.check(L_.fe_electron_classes(_lib.ptr(tab._buf), _lib.ptr(pts_d), npts,
+                                                  _lib.ptr(out), _lib.ptr(ws), ws.numel(), prec,
+                                                  0.0, L, L, None, _lib.stream_ptr()))
+            ms = _median_ms(run, reps, warm=2, flush=flush)
+            row[f"{name}_ms"] = ms
+            row[f"{name}_tflops"] = fl / (ms * 1e-3) / 1e12
+            row[f"{name}_frac"] = fl / (ms * 1e-3) / peak
+        rows.append(row)
+    return rows
 
 
 def hbm_view(traffic, ms):
@@ -138,6 +187,22 @@ def hbm_view(traffic, ms):
     achieved = traffic / (ms * 1e-3) / 1e9
     return {"achieved": achieved, "peak": gbs, "unit": "GB/s", "frac": achieved / gbs,
             "peak_source": src}
+
+
+def build_roofline(wfn, build_ms, peak64, npts):
+    """The table build against the FP64 peak: E-coefficients, Hermite table and
+    G contraction of every primitive pair over the build time.  The point
+    screen is left out of the count: the reference's brute-force screen
+    (8 FLOP per pair and point) is quoted beside it, but the build here prunes
+    it over point-block bounding boxes and does a small fraction of that work."""
+    if build_ms is None:
+        return None
+    fl = build_flops(wfn)
+    npair = build_pairs_count(wfn)
+    return {"ms": build_ms, "primitive_pairs": npair, "flops": fl,
+            "achieved": fl / (build_ms * 1e-3) / 1e12, "peak": peak64 / 1e12, "unit": "TFLOP/s",
+            "frac": fl / (build_ms * 1e-3) / peak64,
+            "bruteforce_screen_flops": 8.0 * npair * npts}
 
 
 def algorithmic_flops(counts, npts):
@@ -287,8 +352,10 @@ def run_ours(args):
     parity = float(np.abs(gt.esp() - g["esp_t12"]).max())
     status = _lib.status(clear=True)
 
-    peak64 = peak_flops(torch, fp64=True)
-    peak32 = peak_flops(torch, fp64=False)
+    peak64 = peak_flops(torch, 1)
+    peak32_scalar = peak_flops(torch, 0)
+    peak32_packed = peak_flops(torch, 2)
+    peak32 = max(peak32_scalar, peak32_packed)
     flops = algorithmic_flops(counts, args.points)
     achieved = flops / (ms_per_step * 1e-3)
     peak = peak32 if prec == "mixed" else peak64
@@ -315,11 +382,17 @@ def run_ours(args):
         "roofline": {"bound": "fp32" if prec == "mixed" else "fp64",
                      "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "peak_source": "measured FMA throughput (fe_peak_run) on this GPU, this run",
+                     "peak_source": ("measured FMA throughput (fe_peak_run) on this GPU, this run: "
+                                     "FP32 the larger of scalar FFMA and packed FFMA2 "
+                                     f"({peak32_scalar / 1e12:.2f} / {peak32_packed / 1e12:.2f} "
+                                     "TFLOP/s), FP64 DFMA"),
                      "flops_per_step": flops,
                      "fp64_path": {"achieved": flops / (ms_fp64 * 1e-3) / 1e12,
                                    "peak": peak64 / 1e12, "frac": flops / (ms_fp64 * 1e-3) / peak64},
-                     "hbm_view": hbm_view(traffic, ms_per_step)},
+                     "hbm_view": hbm_view(traffic, ms_per_step),
+                     "build": build_roofline(wfn, build_ms, peak64, args.points),
+                     "per_class": per_class_rates(torch, tab, pts_d, args.points, flush,
+                                                  peak64, peak32)},
         "gpu_launches": args.steps * launches,
         "parity_frag54_300_max_abs": parity,
         "device_status": status,
@@ -330,6 +403,8 @@ def run_ours(args):
         line["extras"] = run_extras(args, dev, flush)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wfn, basis, P, pts, counts, budget_s=args.cpu_budget)
+        # the reference's own GPU pipeline on the same points, as the GPU comparator
+        line["reference_gpu"] = reference_cuda(wfn, basis, P, pts)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -491,7 +566,8 @@ def cpu_baseline(wfn, basis, P, pts, counts=None, budget_s=20.0, per_class=None)
                        f" on all {len(pts)} points: {t_build:.2f} s; NumPy evaluator (1 thread) "
                        f"timed on {sampled} sampled pairs (<= {per_class} per class) at all "
                        f"points and scaled by class pair counts: {t_eval:.1f} s estimated"),
-            "build_s": t_build, "eval_s_estimated": t_eval, "n_pairs": int(tab.n_pairs)}
+            "build_s": t_build, "eval_s_estimated": t_eval, "n_pairs": int(tab.n_pairs),
+            "sampled_pairs": int(sampled)}
 
 
 def reference_cuda(wfn, basis, P, pts, repeats=5):
@@ -528,21 +604,37 @@ def run_reference(args):
     from fastesp_b200 import synth
     wfn, basis, P, _ = synth.load_workload("frag54", 10, seed=0)
     pts = synth.vdw_surface_points(wfn.symbols, wfn.coords, args.points, seed=1)
-    per_step = []
+    est, wall = [], []
     base = None
     for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
         cb = cpu_baseline(wfn, basis, P, pts, budget_s=2.0, per_class=6)
+        dt = time.perf_counter() - t0
         if i >= args.warmup:
-            per_step.append(len(pts) / cb["value"])
+            est.append(len(pts) / cb["value"])
+            wall.append(dt)
             base = cb
-    ms = 1e3 * statistics.mean(per_step)
-    value = len(pts) / (ms * 1e-3)
+    ms_est = 1e3 * statistics.mean(est)
+    value = len(pts) / (ms_est * 1e-3)
     base = dict(base, value=value)
+    # A step runs the reference's full table build on all points plus its NumPy
+    # evaluator on a bounded sample of pairs (at all points); ms_per_step is that
+    # step's measured wall time.  ``value`` is the whole workload's throughput
+    # estimated from it: the evaluation is exactly linear in the pairs of a
+    # class, so the sampled pairs' time is scaled by the class pair counts.
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "points/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * statistics.mean(wall),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": WORKLOAD, "points_per_gpu": args.points,
                                              "precision": "fp64"},
+            "value_is_estimate": True,
+            "estimate": {"workload_ms_estimated": ms_est,
+                         "how": ("reference build_pairs timed in full; reference NumPy evaluator "
+                                 "timed on 6 sampled pairs per class at all points and scaled "
+                                 "by the class pair counts (its cost per pair is the same "
+                                 "within a class)"),
+                         "scale_factor": base["n_pairs"] / max(1, base.get("sampled_pairs", 1))},
             "cpu_baseline": base,
             "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -553,6 +645,21 @@ def run_reference(args):
     except Exception as e:                      # reported, never fatal for the CPU arm
         line["reference_cuda"] = {"unavailable": f"{type(e).__name__}: {e}"[:200]}
     print(json.dumps(line))
+
+
+def free_port() -> int:
+    import socket
+    with socket.socket() as s_:
+        s_.bind(("127.0.0.1", 0))
+        return s_.getsockname()[1]
+
+
+def launcher_argv(n_gpus: int, argv, port: int) -> list:
+    """This script as ``n_gpus`` ranks of one node under torch.distributed.run
+    (one process per GPU; each reads RANK / LOCAL_RANK / WORLD_SIZE)."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+            f"--nproc-per-node={n_gpus}", "--master-addr=127.0.0.1", f"--master-port={port}",
+            str(Path(__file__).resolve()), *argv]
 
 
 def main():
@@ -572,9 +679,20 @@ def main():
                     help="run one of the extra measurements alone and print its JSON")
     ap.add_argument("--eval-only", action="store_true",
                     help="time only the two evaluators (short run for profiling)")
+    ap.add_argument("--print-ranks", action="store_true",
+                    help="print this process's rank assignment as JSON and exit (no GPU work)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ and not args.only:
+        # --gpus N without a launcher: become N ranks (one per GPU) of this node
+        sys.stdout.flush()
+        os.execv(sys.executable, launcher_argv(args.gpus, sys.argv[1:], free_port()))
+    if args.print_ranks:
+        rank, world, local = rank_info()
+        print(json.dumps({"rank": rank, "local_rank": local, "world_size": world,
+                          "gpus_asked": args.gpus}), flush=True)
+        return
     if args.only:
         import torch
         dev = torch.device("cuda", 0)

@@ -79,10 +79,13 @@ _SIGS = {
     "fe_esp_fp64": (C.c_int, [_P, _P, C.c_int, _P, _P, C.c_size_t, _P]),
     "fe_electron_fp64": (C.c_int, [_P, _P, C.c_int, _P, _P, C.c_size_t, _P]),
     "fe_nuclear_fp64": (C.c_int, [_P, _P, C.c_int, _P, _P, C.c_size_t, _P]),
+    "fe_electron_classes": (C.c_int, [_P, _P, C.c_int, _P, _P, C.c_size_t, C.c_int,
+                                      C.c_double, C.c_int, C.c_int, _P, _P]),
     "fe_esp_mixed": (C.c_int, [_P, _P, C.c_int, _P, _P, C.c_size_t, C.c_double, _P, _P]),
     "fe_electron_mixed": (C.c_int, [_P, _P, C.c_int, _P, _P, C.c_size_t, C.c_double, _P, _P]),
     "fe_boys_fp64": (C.c_int, [_P, C.c_int, C.c_int, _P, _P]),
     "fe_peak_run": (C.c_int, [C.c_int, C.c_longlong, C.c_int, _P, _P]),
+    "fe_wait_selftest": (C.c_int, [C.c_longlong, _P, _P]),
     "fe_esp_fp64_noalloc": (C.c_int, [_P, _P, C.c_int, _P, _P]),
     "fe_noalloc_scratch_bytes": (C.c_size_t, []),
     "fe_field_ws_bytes": (C.c_size_t, [C.c_int]),

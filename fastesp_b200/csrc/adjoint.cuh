@@ -99,6 +99,9 @@ __global__ void __launch_bounds__(NT, MINB) fe_field_f64_kernel(const FeFieldArg
   for (int i = 0; i < total; ++i) {
     if (!pipe.wait(i)) {
       pipe.abort(i);
+      for (int c = 0; c < 4; ++c)
+        fe_poison_row<NP>(a.partial + c * a.plane + size_t(split) * a.ld,
+                          int(blockIdx.x) * (NT * NP) + tid, NT, a.npts);
       return;
     }
     int L, first, n;

@@ -98,7 +98,10 @@ __global__ void __launch_bounds__(128, MINB) fe_batch_f64_kernel(const unsigned 
 #undef FE_CB
       pipe.release(i);
     }
-    if (!ok) return;               // the status word says why; outputs are not valid
+    if (!ok) {                     // the status word says why; the points read NaN
+      fe_poison_row<NP>(partial + m.base + size_t(m.row0[L] + item.part) * m.ld, p0, NT, m.npts);
+      return;
+    }
     if (L < LLO || L > LHI) fe_flag(FE_ST_BADCLASS);
 #pragma unroll
     for (int j = 0; j < NP; ++j) {

@@ -50,16 +50,33 @@ FE_DEV bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   return ok != 0;
 }
 
-// Wait for phase ``parity`` of ``bar`` for at most ~1 s of SM clock (and a hard
-// iteration cap).  Returns false (and flags FE_ST_TIMEOUT) if it gave up.
-FE_DEV bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+// Wait for phase ``parity`` of ``bar`` for at most ``cycles`` SM clocks (and a
+// hard iteration cap).  Returns false (and flags FE_ST_TIMEOUT) if it gave up.
+FE_DEV bool mbar_wait_limited(uint64_t* bar, unsigned parity, long long cycles) {
   const long long t0 = clock64();
   for (unsigned it = 0; it < (1u << 26); ++it) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (clock64() - t0 > 2000000000LL) break;
+    if (clock64() - t0 > cycles) break;
   }
   fe_flag(FE_ST_TIMEOUT);
   return false;
+}
+
+// The evaluators' wait: about 1 s of SM clock.
+FE_DEV bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+  return mbar_wait_limited(bar, parity, 2000000000LL);
+}
+
+// A block whose bounded wait gave up has incomplete sums: it writes NaN to its
+// points' entries of its partial row (points p0 + j * stride, j < NP), so the
+// reduction gives NaN for those points instead of a partial or stale value.
+template <int NP>
+FE_DEV void fe_poison_row(double* row, int p0, int stride, int npts) {
+#pragma unroll
+  for (int j = 0; j < NP; ++j) {
+    const int p = p0 + j * stride;
+    if (p < npts) row[p] = __longlong_as_double(0x7ff8000000000000LL);
+  }
 }
 
 // 1-D TMA bulk copy global -> shared, completing on ``bar`` (no multicast).

@@ -35,6 +35,7 @@ struct FeEvalArgs {
   int nsplit;
   double* partial;                 // [nsplit][ld] partial electron sums of this kernel
   int ld;
+  int lmin, lmax;                  // classes evaluated (a sub-range for per-class timing)
 };
 
 // Pairs of class L per stage / tile.
@@ -254,13 +255,15 @@ __global__ void __launch_bounds__(NT, MINB) fe_eval_f64_kernel(const FeEvalArgs 
   }
   FeTilePipe pipe{a.table, fe_c_tile64, fe_c_rec64, hdr->off64, 8, fe_smem, full_bar, &w};
   int Lrow, part, nparts;
-  fe_class_rows(hdr, LLO, LHI, a.nsplit, split, Lrow, part, nparts);
+  fe_class_rows(hdr, max(LLO, a.lmin), min(LHI, a.lmax), a.nsplit, split, Lrow, part, nparts);
   if (Lrow >= 0) pipe.start(hdr, part, nparts, Lrow, Lrow);
   else pipe.start(hdr, 0, 1, 1, 0);                     // idle row: no tiles
   const int total = w.total;
   for (int i = 0; i < total; ++i) {
     if (!pipe.wait(i)) {
       pipe.abort(i);
+      fe_poison_row<NP>(a.partial + size_t(split) * a.ld, int(blockIdx.x) * (NT * NP) + tid, NT,
+                        a.npts);
       return;
     }
     int L, first, n;

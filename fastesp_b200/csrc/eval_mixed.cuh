@@ -53,6 +53,7 @@ struct FeMixedArgs {
   unsigned long long* n64;       // optional: count of (pair, warp) FP64 evaluations
   unsigned* mask;                // routing mask (one bit per pair and warp)
   long long mask_words;          // its capacity in 32-bit words
+  int lmin, lmax;                // classes evaluated (a sub-range for per-class timing)
 };
 
 __constant__ int fe_c_tile32[FE_NCLASS] = {
@@ -274,7 +275,7 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
   }
   FeTilePipe pipe{a.table, fe_c_tile32, fe_c_rec32, hdr->off32, 4, fe_smem, full_bar, &w};
   int Lrow, part, nparts;
-  fe_class_rows(hdr, LLO, LHI, a.nsplit, blockIdx.y, Lrow, part, nparts);
+  fe_class_rows(hdr, max(LLO, a.lmin), min(LHI, a.lmax), a.nsplit, blockIdx.y, Lrow, part, nparts);
   if (Lrow >= 0) pipe.start(hdr, part, nparts, Lrow, Lrow, 32);
   else pipe.start(hdr, 0, 1, 1, 0, 32);                 // idle row: no tiles
   const int total = w.total;
@@ -288,6 +289,7 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
   for (int i = 0; i < total; ++i) {
     if (!pipe.wait(i)) {
       pipe.abort(i);
+      fe_poison_row<NP>(a.partial + size_t(blockIdx.y) * a.ld, p0, NT, a.npts);
       return;
     }
     int L, first, n;
@@ -347,7 +349,7 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_fix64_kernel(const FeM
   const long long warp0 = (long long)blockIdx.x * NW;
   unsigned n64 = 0;
   int L, part, nparts;
-  fe_class_rows(hdr, LLO, LHI, a.nsplit, blockIdx.y, L, part, nparts);
+  fe_class_rows(hdr, max(LLO, a.lmin), min(LHI, a.lmax), a.nsplit, blockIdx.y, L, part, nparts);
   if ((warp0 + NW) * w.wtotal > a.mask_words) {
     if (tid == 0) fe_flag(FE_ST_OVERFLOW);
     L = -1;

@@ -2,6 +2,7 @@
 //
 // Single translation unit: the device code lives in the included headers,
 // this file holds the host-side planning and the extern "C" entry points.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -574,7 +575,8 @@ namespace {
 
 int eval_launch(const char* who, const void* d_table, const double* d_pts, int n_pts,
                 double* d_out, void* d_ws, size_t ws_bytes, int out_mode, int prec,
-                double tau, unsigned long long* d_n64, cudaStream_t st) {
+                double tau, unsigned long long* d_n64, cudaStream_t st, int lmin = 0,
+                int lmax = FE_NCLASS - 1) {
   if (n_pts < 0) return fail(FE_ERR_ARG, "%s: n_pts < 0", who);
   if (n_pts == 0) return FE_OK;
   if (!d_table || !d_pts || !d_out) return fail(FE_ERR_ARG, "%s: null argument", who);
@@ -596,6 +598,8 @@ int eval_launch(const char* who, const void* d_table, const double* d_pts, int n
     a.pts = d_pts;
     a.npts = n_pts;
     a.ld = g.ld;
+    a.lmin = lmin;
+    a.lmax = lmax;
     auto k0 = fe_eval_f64_kernel<kNP64, kEvalThreads, kMinB64, 0, FE_LSPLIT>;
     auto k1 = fe_eval_f64_kernel<kNP64, kEvalThreads, 1, FE_LSPLIT + 1, FE_NCLASS - 1>;
     a.nsplit = g.split[0];
@@ -620,6 +624,8 @@ int eval_launch(const char* who, const void* d_table, const double* d_pts, int n
     a.n64 = d_n64;
     a.mask = reinterpret_cast<unsigned*>(static_cast<unsigned char*>(d_ws) + rows_bytes);
     a.mask_words = static_cast<long long>((ws_bytes - rows_bytes) / 4);
+    a.lmin = lmin;
+    a.lmax = lmax;
     auto f0 = fe_eval_f32_kernel<kMinB32Lo, 0, FE_MXSPLIT>;
     auto f0b = fe_eval_f32_kernel<kMinB32, FE_MXSPLIT + 1, FE_LSPLIT>;
     auto f1 = fe_eval_f32_kernel<1, FE_LSPLIT + 1, FE_NCLASS - 1>;
@@ -681,6 +687,19 @@ int fe_electron_mixed(const void* d_table, const double* d_pts, int n_pts, doubl
                      d_n64, st);
 }
 
+int fe_electron_classes(const void* d_table, const double* d_pts, int n_pts, double* d_out,
+                        void* d_ws, size_t ws_bytes, int precision, double tau, int lmin,
+                        int lmax, unsigned long long* d_n64, cudaStream_t st) {
+  if (precision != 0 && precision != 1)
+    return fail(FE_ERR_ARG, "fe_electron_classes: precision must be 0 (FP64) or 1 (mixed)");
+  if (lmin < 0 || lmax >= FE_NCLASS || lmin > lmax)
+    return fail(FE_ERR_ARG, "fe_electron_classes: class range %d..%d outside 0..%d", lmin, lmax,
+                FE_NCLASS - 1);
+  if (!(tau > 0.0)) tau = kTauDefault;
+  return eval_launch("fe_electron_classes", d_table, d_pts, n_pts, d_out, d_ws, ws_bytes, 1,
+                     precision, tau, d_n64, st, lmin, lmax);
+}
+
 int fe_nuclear_fp64(const void* d_table, const double* d_pts, int n_pts, double* d_out,
                     void* d_ws, size_t ws_bytes, cudaStream_t st) {
   (void)d_ws;
@@ -725,7 +744,10 @@ extern "C" int fe_boys_fp64(const double* d_T, int n, int mmax, double* d_F, cud
 
 // ---------------------------------------------------------------------------
 // FMA throughput probe: the FP64 / FP32 pipe peak used as the roofline
-// denominator (8 independent FMA chains per thread, no memory traffic).
+// denominator (8 independent FMA chains per thread, no memory traffic).  The
+// packed form issues FP32x2 fused multiply-adds (two lanes per instruction),
+// as the mixed evaluator does, so it needs half the issue slots of the scalar
+// form for the same FMA-pipe work.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(256) fe_peak_kernel(long long iters, T* out) {
@@ -743,13 +765,58 @@ __global__ void __launch_bounds__(256) fe_peak_kernel(long long iters, T* out) {
   if (threadIdx.x == 0) out[blockIdx.x] = s;
 }
 
-extern "C" int fe_peak_run(int fp64, long long iters, int blocks, void* d_out, cudaStream_t st) {
-  if (iters <= 0 || blocks <= 0 || !d_out) return fail(FE_ERR_ARG, "fe_peak_run: bad argument");
-  if (fp64)
+__global__ void __launch_bounds__(256) fe_peak2_kernel(long long iters, float* out) {
+  float2 a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = make_float2(float(threadIdx.x + k) * 1e-6f, float(k) * 1e-6f);
+  const float2 b = fe_f2(0.9999999f), c = fe_f2(1e-7f);
+#pragma unroll 4
+  for (long long it = 0; it < iters; ++it)
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = fe_fma(a[k], b, c);
+  float s = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += a[k].x + a[k].y;
+  if (threadIdx.x == 0) out[blockIdx.x] = s;
+}
+
+extern "C" int fe_peak_run(int kind, long long iters, int blocks, void* d_out, cudaStream_t st) {
+  if (iters <= 0 || blocks <= 0 || !d_out || kind < 0 || kind > 2)
+    return fail(FE_ERR_ARG, "fe_peak_run: bad argument");
+  if (kind == 1)
     fe_peak_kernel<double><<<blocks, 256, 0, st>>>(iters, static_cast<double*>(d_out));
-  else
+  else if (kind == 0)
     fe_peak_kernel<float><<<blocks, 256, 0, st>>>(iters, static_cast<float*>(d_out));
+  else
+    fe_peak2_kernel<<<blocks, 256, 0, st>>>(iters, static_cast<float*>(d_out));
   FE_CUDA(cudaGetLastError());
+  return FE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Self-test of the bounded-wait path: one thread waits on an mbarrier that no
+// thread arrives on and no copy targets, so the wait must give up after
+// ``cycles`` SM clocks, flag FE_ST_TIMEOUT and let the kernel return.
+// ---------------------------------------------------------------------------
+__global__ void fe_wait_selftest_kernel(long long cycles, int* done) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  mbar_fence_init();
+  const bool got = mbar_wait_limited(&bar, 0, cycles);
+  *done = got ? 1 : 2;
+}
+
+extern "C" int fe_wait_selftest(long long cycles, int* d_done, cudaStream_t st) {
+  if (cycles <= 0 || cycles > 4000000000LL || !d_done)
+    return fail(FE_ERR_ARG, "fe_wait_selftest: cycles must be in 1..4e9 and d_done non-null");
+  fe_wait_selftest_kernel<<<1, 32, 0, st>>>(cycles, d_done);
+  FE_CUDA(cudaGetLastError());
+  FE_CUDA(cudaStreamSynchronize(st));
+  unsigned v = 0;
+  FE_CUDA(cudaMemcpyFromSymbol(&v, fe_status_word, sizeof v));
+  if (v & FE_ST_TIMEOUT)
+    return fail(FE_ERR_DEVICE, "fe_wait_selftest: device status 0x%x (a bounded wait gave up)", v);
   return FE_OK;
 }
 
@@ -771,23 +838,61 @@ extern "C" int fe_peak_run(int fp64, long long iters, int blocks, void* d_out, c
 static __device__ __align__(256) unsigned char fe_noalloc_scratch[FE_NOALLOC_SCRATCH_BYTES];
 
 namespace {
+// Device address of the scratch array, per device, with the ID of the context
+// it was resolved in.  The host-side symbol is only a stand-in, never a device
+// address, so the address comes from cudaGetSymbolAddress once per device; a
+// device reset replaces the device's context (and may move the array), which
+// the context ID shows, and the address is then resolved again.
+struct NoallocSlot {
+  void* ptr = nullptr;
+  unsigned long long ctx_id = 0;
+};
 std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[FE_NOALLOC_MAX_DEVICES] = {};
+NoallocSlot g_noalloc[FE_NOALLOC_MAX_DEVICES];
 
-// Device address of the scratch array on the current device; resolved once per
-// device (the host-side symbol is only a stand-in, never a device address).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// ID of the calling thread's current context (0 when none is current), from
+// the driver's entry points as the runtime hands them out (no link to libcuda).
+unsigned long long current_ctx_id() {
+  static CtxGetCurrentFn get_cur = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_cur = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+  });
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_cur || !get_id || get_cur(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// The scratch array's device address on the current device.
 int noalloc_scratch(void** out) {
   int dev = 0;
   FE_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= FE_NOALLOC_MAX_DEVICES)
     return fail(FE_ERR_UNSUPPORTED, "fe_esp_fp64_noalloc: device ordinal %d too large", dev);
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
+  NoallocSlot& s = g_noalloc[dev];
+  const unsigned long long id = current_ctx_id();
+  if (!s.ptr || id == 0 || id != s.ctx_id) {
     void* p = nullptr;
     FE_CUDA(cudaGetSymbolAddress(&p, fe_noalloc_scratch));
-    g_noalloc_ptr[dev] = p;
+    s.ptr = p;
+    s.ctx_id = current_ctx_id();        // the lookup made the device's context current
   }
-  *out = g_noalloc_ptr[dev];
+  *out = s.ptr;
   return FE_OK;
 }
 }  // namespace

@@ -160,3 +160,17 @@ def eval_flops(L: int) -> int:
     nt = n_terms(L)
     nm = len(mono_schedule(L)[0])
     return 2 * nt + (nm - 1) + 14 + 3 * L
+
+
+def build_flops(la: int, lb: int) -> int:
+    """Algorithmic floating-point operations of building one primitive pair of
+    shells with angular momenta (la, lb), without the point screen:
+    3 (la+1)(lb+1)(L+1) * 4 for the three axes' E-coefficients, ncart(la)
+    ncart(lb) (L+1)^3 * 2 for the density-weighted Hermite table and
+    2 nnz(M0) for the G contraction -- the steps of the reference's pair
+    construction (fastesp/esp.py:108-257, fastesp/native/build_pairs.cpp:237-316).
+    """
+    L = la + lb
+    nc = lambda l: (l + 1) * (l + 2) // 2  # noqa: E731
+    nnz = sum(len(r) for r in class_terms(L)[1])
+    return 3 * (la + 1) * (lb + 1) * (L + 1) * 4 + nc(la) * nc(lb) * (L + 1) ** 3 * 2 + 2 * nnz

@@ -4,7 +4,10 @@
 the reference's point scripts do (benchmarks/make_points.py:22-58,
 examples/vdw_surface_esp.py:38-52): per atom a share of Fibonacci-sphere
 candidates proportional to its sphere area, oversampled, kept when outside
-every other sphere, then a seeded subset.  ``grid_points`` takes a seeded
+every other sphere, then a seeded subset (``mode="reference"`` draws exactly
+as those scripts do; the default, used for the benchmark workloads at 1.4x
+radii, retries with more candidates when too few survive and keeps the drawn
+points in candidate order).  ``grid_points`` takes a seeded
 subset of a cubic grid around the molecule and drops points near nuclei.
 
 The O(N_candidates x N_atoms) candidate generation and exposure test run as
@@ -55,9 +58,16 @@ def surface_candidates(symbols, coords, counts, slack=1e-9, scale=1.4, device=No
 
 
 def surface_points(symbols, coords, n_points: int, seed: int = 0, scale: float = 1.4,
-                   device=None):
-    """(n_points, 3) Bohr on the exposed ``scale`` x Bondi surface, as a CUDA tensor."""
+                   mode: str = "retry", device=None):
+    """(n_points, 3) Bohr on the exposed ``scale`` x Bondi surface, as a CUDA tensor.
+
+    ``mode`` as in :func:`fastesp_b200.synth.vdw_surface_points`: "reference"
+    draws exactly as the reference's point scripts (one candidate pass, seeded
+    draw in the generator's order, all candidates if fewer; they use scale
+    1.0), "retry" as the benchmark workloads."""
     import torch
+    if mode not in ("retry", "reference"):
+        raise ValueError(f"mode must be 'retry' or 'reference', got {mode!r}")
     rad = np.array([scale * BONDI[s] / BOHR for s in symbols])
     share = rad ** 2 / (rad ** 2).sum()
     rng = np.random.default_rng(seed)
@@ -65,10 +75,15 @@ def surface_points(symbols, coords, n_points: int, seed: int = 0, scale: float =
     while True:
         counts = [int(np.ceil(n_points * share[a] * over)) + 50 for a in range(len(symbols))]
         cand = surface_candidates(symbols, coords, counts, scale=scale, device=device)
-        if cand.shape[0] >= n_points:
+        if cand.shape[0] >= n_points or mode == "reference":
             break
         over *= 2.0
-    sel = np.sort(rng.choice(cand.shape[0], n_points, replace=False))
+    if mode == "reference":
+        if cand.shape[0] <= n_points:
+            return cand.contiguous()
+        sel = rng.choice(cand.shape[0], size=n_points, replace=False)
+    else:
+        sel = np.sort(rng.choice(cand.shape[0], n_points, replace=False))
     return cand[torch.as_tensor(sel, device=cand.device)].contiguous()
 
 

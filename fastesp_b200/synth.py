@@ -206,8 +206,21 @@ def fibonacci_sphere(n: int) -> np.ndarray:
 
 
 def vdw_surface_points(symbols, coords, n_points: int, seed: int = 0,
-                       scale: float = 1.4) -> np.ndarray:
-    """~uniform points on the exposed union of ``scale`` x Bondi spheres (Bohr)."""
+                       scale: float = 1.4, mode: str = "retry") -> np.ndarray:
+    """~uniform points on the exposed union of ``scale`` x Bondi spheres (Bohr).
+
+    Per atom, ceil(3 n_points share) + 50 Fibonacci-sphere candidates (share:
+    the atom's fraction of the total sphere area), kept when no other sphere
+    covers them.  ``mode="reference"`` is the reference's point scripts
+    exactly (examples/vdw_surface_esp.py:38-52, benchmarks/make_points.py:
+    40-58, which use scale 1.0): one candidate pass, then ``n_points`` of them
+    drawn by the seeded generator in its (unsorted) order, or all of them if
+    there are fewer.  ``mode="retry"`` (the benchmark workloads) doubles the
+    oversampling until there are enough candidates and keeps the drawn ones in
+    candidate order.
+    """
+    if mode not in ("retry", "reference"):
+        raise ValueError(f"mode must be 'retry' or 'reference', got {mode!r}")
     rad = np.array([scale * BONDI[s] / BOHR for s in symbols])
     share = rad ** 2 / (rad ** 2).sum()
     rng = np.random.default_rng(seed)
@@ -220,9 +233,13 @@ def vdw_surface_points(symbols, coords, n_points: int, seed: int = 0,
             d = np.linalg.norm(p[:, None, :] - coords[None, :, :], axis=2)
             cand.append(p[(d >= rad[None, :] - 1e-9).all(axis=1)])
         cand = np.concatenate(cand)
-        if len(cand) >= n_points:
+        if len(cand) >= n_points or mode == "reference":
             break
         over *= 2.0
+    if mode == "reference":
+        if len(cand) > n_points:
+            cand = cand[rng.choice(len(cand), size=n_points, replace=False)]
+        return np.ascontiguousarray(cand)
     sel = np.sort(rng.choice(len(cand), n_points, replace=False))
     return np.ascontiguousarray(cand[sel])
 

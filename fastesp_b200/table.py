@@ -436,13 +436,21 @@ class PairTable:
         reference builders write); the class is identified by the term count.
         """
         d = Path(path).read_bytes()
+        if len(d) < 4 * HEADER_FIELDS:
+            raise _lib.FeError(3, f"{path}: {len(d)} bytes, shorter than the pairs.bin header")
         n, nt, npt, nat, _ = struct.unpack_from("<8i", d, 0)[:5]
+        if min(n, nt, npt, nat) < 0:
+            raise _lib.FeError(1, f"{path}: negative count in the pairs.bin header")
         o = 4 * HEADER_FIELDS
 
         def rd(dt, count):
             nonlocal o
+            nb = np.dtype(dt).itemsize * count
+            if o + nb > len(d):
+                raise _lib.FeError(3, f"{path}: truncated pairs.bin ({len(d)} bytes; the header's "
+                                      f"counts need more than {o + nb})")
             a = np.frombuffer(d, dtype=dt, count=count, offset=o)
-            o += np.dtype(dt).itemsize * count
+            o += nb
             return a
 
         f = {k: rd(np.float64, n) for k in ("pp_exp", "pp_cx", "pp_cy", "pp_cz", "pp_K")}

@@ -164,6 +164,15 @@ int fe_electron_mixed(const void* d_table, const double* d_pts, int n_pts, doubl
 int fe_electron_fp64(const void* d_table, const double* d_pts, int n_pts, double* d_out,
                      void* d_ws, size_t ws_bytes, cudaStream_t stream);
 
+/* The electron part of the pairs of classes lmin..lmax only (no counterpart in
+ * the reference): FP64 (precision 0, workspace fe_eval_ws_bytes) or mixed
+ * (precision 1, workspace fe_eval_ws_bytes_mixed, routing threshold tau as in
+ * fe_esp_mixed).  The sum over a partition of 0..FE_NCLASS-1 into ranges is the
+ * full electron part; used to time and rate each class on its own. */
+int fe_electron_classes(const void* d_table, const double* d_pts, int n_pts, double* d_out,
+                        void* d_ws, size_t ws_bytes, int precision, double tau, int lmin,
+                        int lmax, unsigned long long* d_n64, cudaStream_t stream);
+
 /* The nuclear part alone, sum_A Z_A/|C-R_A| (fastesp/table.py:95-100); the
  * workspace arguments are unused and may be null. */
 int fe_nuclear_fp64(const void* d_table, const double* d_pts, int n_pts, double* d_out,
@@ -179,14 +188,19 @@ int fe_boys_fp64(const double* d_T, int n, int mmax, double* d_F, cudaStream_t s
  * binding of the reference's table-and-points-in / potentials-out interface --
  * the partial sums live in a file-scope device array of
  * fe_noalloc_scratch_bytes() (16 MiB) that every GPU loading the library keeps
- * until the process exits.  Point counts whose scratch would exceed it are
- * refused with FE_ERR_SIZE (about 10^6 points on a 148-SM B200).  Allocates
- * nothing: no cudaMalloc, cudaFree or allocating library routine.  The first
- * call on a device looks up the array's device address (cudaGetSymbolAddress)
- * and should come before any stream capture.  All calls share the array and
- * every partial sum it holds is rewritten before it is read, so nothing needs
- * clearing, but calls whose executions overlap on the GPU (other streams, other
- * host threads) race on it and must be serialised by the caller. */
+ * until the process exits.  A point count n fits when fe_eval_ws_bytes(n) <=
+ * fe_noalloc_scratch_bytes(): up to 232,992 points on a 148-SM B200 (large
+ * counts need 9 FP64 rows of the padded point count); larger counts are
+ * refused with FE_ERR_SIZE before anything is launched.  Allocates nothing: no
+ * cudaMalloc, cudaFree or allocating library routine.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) and should
+ * come before any stream capture; the address is looked up again after a
+ * device reset (a new context).  All calls share the array and every partial
+ * sum it holds is rewritten before it is read, so nothing needs clearing: a
+ * block whose bounded wait gave up writes NaN for its points, and the status
+ * word (fe_status) records it.  Calls whose executions overlap on the GPU
+ * (other streams, other host threads) race on the array and must be
+ * serialised by the caller. */
 int fe_esp_fp64_noalloc(const void* d_table, const double* d_pts, int n_pts, double* d_out,
                         cudaStream_t stream);
 size_t fe_noalloc_scratch_bytes(void);
@@ -272,11 +286,23 @@ int fe_grid_points(const double* d_xyz, int natom, double exclude, const long lo
                    double* d_out, long long cap, int* d_count, void* d_ws, size_t ws_bytes,
                    cudaStream_t stream);
 
+/* Self-test of the bounded waits (no counterpart in the reference, whose
+ * tools exit on errors): one block waits on an mbarrier that nothing arrives on
+ * and no copy targets, for at most ``cycles`` SM clocks (1..4e9).  The wait
+ * gives up, sets bit 1 (FE_ST_TIMEOUT) of the status word and the kernel
+ * returns normally, so the context stays usable; *d_done is 2 (gave up) or
+ * 1 (completed).  Synchronises ``stream`` and returns FE_ERR_DEVICE when the
+ * status word has the timeout bit, as every caller should treat it.  The bit
+ * stays set until fe_status(..., 1) clears it. */
+int fe_wait_selftest(long long cycles, int* d_done, cudaStream_t stream);
+
 /* FMA throughput probe (no counterpart in the reference): ``blocks`` blocks of
- * 256 threads each run ``iters`` iterations of 8 independent FMA chains in FP64
- * (fp64 != 0) or FP32, writing one value per block to d_out.  Timed by the
- * caller; FLOPs = 16 * iters * 256 * blocks.  Used as the FP64/FP32 roofline. */
-int fe_peak_run(int fp64, long long iters, int blocks, void* d_out, cudaStream_t stream);
+ * 256 threads each run ``iters`` iterations of 8 independent FMA chains, in
+ * FP32 (kind 0), FP64 (kind 1) or packed FP32x2 (kind 2: two lanes per
+ * instruction, as the mixed evaluator issues them), writing one value per
+ * block to d_out.  Timed by the caller; FLOPs = 16 * iters * 256 * blocks
+ * (twice that for kind 2).  Used as the FP64/FP32 roofline. */
+int fe_peak_run(int kind, long long iters, int blocks, void* d_out, cudaStream_t stream);
 
 #ifdef __cplusplus
 }

@@ -1,6 +1,9 @@
 """Generate the golden fixtures by running the reference (ZidongS/fastesp) itself.
 
-    python tests/golden/make_golden.py [--reference /root/reference] [--quick]
+    python tests/golden/make_golden.py [--reference DIR] [--quick]
+
+DIR defaults to $FASTESP_REFERENCE, else a checkout named ``reference`` beside
+this repository.
 
 The reference's Python package is imported read-only from its checkout, and its
 C++ table builder is run from ``oracle/_ref/build_pairs`` (built from the
@@ -20,10 +23,14 @@ Fixtures
                       builder's kept-pair count and ESP (its screening rule)
   frag54_300.npz      54-atom system at 300 vdW points (the MOLDEN file is
                       regenerated from its seed; ESP at tol 1e-12 and 0)
+  ref_points.npz      the reference's vdW-surface sampler
+                      (examples/vdw_surface_esp.py: vdw_surface_points) on the
+                      small system and the 54-atom system, several seeds
 """
 from __future__ import annotations
 
 import argparse
+import os
 import subprocess
 import sys
 import tempfile
@@ -38,9 +45,11 @@ ROOT = HERE.parents[1]
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("FASTESP_REFERENCE")
+                    or str(ROOT.parent / "reference"))
     ap.add_argument("--quick", action="store_true", help="skip the 54-atom fixture")
-    ap.add_argument("--only", default="", help="comma list: boys,pair_types,prim,systems,frag54")
+    ap.add_argument("--only", default="",
+                    help="comma list: boys,pair_types,prim,systems,frag54,points")
     a = ap.parse_args()
     sys.path.insert(0, a.reference)
     sys.path.insert(0, str(ROOT))
@@ -71,7 +80,24 @@ def main() -> int:
             return float(mp.gammainc(a_, 0, mp.mpf(t)) / (2 * mp.power(mp.mpf(t), a_)))
         F_exact = np.array([[exact(int(m), float(t)) for t in T] for m in ms[:10]])
         np.savez_compressed(HERE / "boys.npz", T=T, m=ms, F=F, F_exact=F_exact)
-    if not want("pair_types") and not want("prim") and not want("systems") and not want("frag54"):
+    # ---- the reference's vdW-surface sampler ---------------------------------
+    if want("points"):
+        import importlib.util
+        spec = importlib.util.spec_from_file_location(
+            "ref_vdw_surface_esp", Path(a.reference) / "examples" / "vdw_surface_esp.py")
+        ex = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(ex)
+        out = {}
+        with tempfile.TemporaryDirectory() as td:
+            cases = (("small", synth.make_system("small", 0), ((300, 0), (300, 5))),
+                     ("frag54", synth.make_system("frag54", 0), ((3000, 0), (2000, 20260909))))
+            for tag, sysm, runs in cases:
+                wfn = R.read_molden(sysm.write(Path(td) / f"{tag}.molden"))
+                for n, seed in runs:
+                    out[f"{tag}_{n}_{seed}"] = ex.vdw_surface_points(wfn, n, seed=seed)
+        np.savez_compressed(HERE / "ref_points.npz", **out)
+        print("ref_points:", {k: v.shape for k, v in out.items()})
+    if not any(want(k) for k in ("pair_types", "prim", "systems", "frag54")):
         return 0
 
     # ---- per-L contraction tables -------------------------------------------

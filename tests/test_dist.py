@@ -68,3 +68,32 @@ def test_rank_point_sets_differ(small_system):
     a = rank_points(wfn.symbols, wfn.coords, 50, 0)
     b = rank_points(wfn.symbols, wfn.coords, 50, 1)
     assert a.shape == b.shape == (50, 3) and not np.array_equal(a, b)
+
+
+def test_bench_launches_one_rank_per_gpu():
+    """``bench.py --gpus 2`` without a launcher re-executes itself under
+    torch.distributed.run as two ranks; each sees its own RANK / LOCAL_RANK
+    (checked here without touching CUDA)."""
+    import json
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT")}
+    r = subprocess.run([sys.executable, str(root / "bench.py"), "--gpus", "2", "--print-ranks"],
+                       capture_output=True, text=True, timeout=180, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    ranks = sorted((json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")),
+                   key=lambda d: d["rank"])
+    assert [(d["rank"], d["local_rank"], d["world_size"]) for d in ranks] == [(0, 0, 2), (1, 1, 2)]
+
+
+def test_launcher_command_line():
+    import sys
+    sys.path.insert(0, str(__import__("pathlib").Path(__file__).resolve().parents[1]))
+    import bench
+    argv = bench.launcher_argv(4, ["--gpus", "4", "--steps", "5"], 29512)
+    assert argv[1:3] == ["-m", "torch.distributed.run"]
+    assert "--nproc-per-node=4" in argv and "--master-addr=127.0.0.1" in argv
+    assert "--master-port=29512" in argv and argv[-4:] == ["--gpus", "4", "--steps", "5"]

@@ -1,0 +1,118 @@
+"""The headline workload pinned to the reference itself at full size.
+
+The 54-atom l<=3 system (molecule seed 0) at the benchmark's 30000 vdW-surface
+points (seed 1), screening tol 1e-12.  The reference's own C++ table builder
+(fastesp/native/build_pairs.cpp) and FP64 CUDA evaluator
+(fastesp/native/esp_gpu.cu), compiled from its sources into oracle/_ref by
+oracle/Makefile, run on the same basis.bin; this package's GPU builder and
+evaluators must reproduce them:
+
+(a) the C++ builder's screen (build_pairs.cpp:318-328, ``rule="native"``)
+    keeps exactly the same pairs, class by class, in the same order;
+(b) the G coefficients of both tables agree to 1e-13 of the class's largest;
+(c) the FP64 path agrees with the reference's evaluator run on the
+    reference's own pairs.bin at all 30000 points to 1e-10 a.u.;
+(d) the mixed-precision path is within 1e-6 a.u. of that same output;
+(e) the table the benchmark times (the NumPy rule, fastesp/table.py:190-194)
+    differs from it only by pairs screened out below tol: within 1e-9 a.u.
+
+Skipped when the reference binaries were not built (the reference checkout
+is needed to build them); nothing here reads the reference checkout.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from fastesp_b200 import _lib, basis_payload, build_table, synth, write_basis_payload
+from fastesp_b200.table import PairTable
+
+pytestmark = pytest.mark.gpu
+REF = Path(__file__).resolve().parents[1] / "oracle" / "_ref"
+BUILD_PAIRS, ESP_GPU = REF / "build_pairs", REF / "esp_gpu"
+NPTS = 30000
+
+
+@pytest.fixture(scope="module")
+def headline(frag54, tmp_path_factory):
+    if not (BUILD_PAIRS.exists() and ESP_GPU.exists()):
+        pytest.skip("oracle/_ref/build_pairs or esp_gpu not built")
+    wfn, basis, P = frag54
+    pts = synth.vdw_surface_points(wfn.symbols, wfn.coords, NPTS, seed=1)
+    td = tmp_path_factory.mktemp("headline")
+    bb, pb, out = td / "basis.bin", td / "pairs.bin", td / "esp.txt"
+    write_basis_payload(bb, basis_payload(wfn, basis, P, pts))
+    env = dict(os.environ, OMP_NUM_THREADS=str(len(os.sched_getaffinity(0))))
+    r = subprocess.run([str(BUILD_PAIRS), str(bb), str(pb), "1e-12"], capture_output=True,
+                       text=True, timeout=900, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    r = subprocess.run([str(ESP_GPU), str(pb), str(out), "--repeats", "1", "--quiet"],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    ref_v = np.loadtxt(out, skiprows=1)
+    np.testing.assert_array_equal(ref_v[:, :3].shape, (NPTS, 3))
+    assert np.abs(ref_v[:, :3] - pts).max() < 1e-11        # printed with 12 decimals
+    _lib.status(clear=True)
+    yield dict(wfn=wfn, basis=basis, P=P, pts=pts, ref_table=PairTable.read(pb),
+               ref_esp=ref_v[:, 3])
+    assert _lib.status(clear=True) == 0, "a kernel reported a device-side failure"
+
+
+@pytest.fixture(scope="module")
+def native_table(headline):
+    h = headline
+    return build_table(h["wfn"], h["basis"], h["P"], h["pts"], tol=1e-12, rule="native")
+
+
+def test_native_rule_keeps_the_reference_pairs(headline, native_table):
+    ref = headline["ref_table"]
+    assert native_table.counts == ref.counts
+    assert native_table.n_pairs == ref.n_pairs
+    for L, c in enumerate(ref.counts):
+        if not c:
+            continue
+        a, b = native_table.records(L)[:, :5], ref.records(L)[:, :5]
+        np.testing.assert_array_equal(a[:, 0], b[:, 0])                  # p = a + b
+        np.testing.assert_allclose(a[:, 1:4], b[:, 1:4], rtol=0, atol=1e-13)   # P
+        np.testing.assert_allclose(a[:, 4], b[:, 4], rtol=1e-14, atol=0)       # K
+
+
+def test_native_rule_coefficients_match(headline, native_table):
+    ref = headline["ref_table"]
+    for L, c in enumerate(ref.counts):
+        if not c:
+            continue
+        g, gr = native_table.coefficients(L), ref.coefficients(L)
+        scale = np.abs(gr).max()
+        assert np.abs(g - gr).max() <= 1e-13 * scale, (L, np.abs(g - gr).max() / scale)
+
+
+def test_fp64_matches_reference_evaluator(headline, native_table):
+    got = native_table.esp(headline["pts"])
+    err = np.abs(got - headline["ref_esp"]).max()
+    print(f"FP64 vs reference esp_gpu at {NPTS} points: max {err:.2e} a.u.")
+    assert err <= 1e-10
+    # the reference's own table evaluated here: the same values again
+    got_ref_tab = headline["ref_table"].esp(headline["pts"])
+    assert np.abs(got_ref_tab - headline["ref_esp"]).max() <= 1e-10
+
+
+def test_mixed_matches_reference_evaluator(headline, native_table):
+    got = native_table.esp(headline["pts"], precision="mixed")
+    d = np.abs(got - headline["ref_esp"])
+    print(f"mixed vs reference esp_gpu at {NPTS} points: max {d.max():.2e}, "
+          f"rms {np.sqrt((d ** 2).mean()):.2e} a.u.")
+    assert d.max() <= 1e-6
+
+
+def test_benchmark_table_within_screening_of_reference(headline):
+    h = headline
+    tab = build_table(h["wfn"], h["basis"], h["P"], h["pts"], tol=1e-12)     # NumPy rule
+    err = np.abs(tab.esp(h["pts"]) - h["ref_esp"]).max()
+    print(f"NumPy-rule table ({tab.n_pairs} pairs) vs reference ({h['ref_table'].n_pairs}): "
+          f"max {err:.2e} a.u.")
+    assert err <= 1e-9

@@ -45,3 +45,19 @@ def test_gpu_prepared_inputs_give_reference_values(small_system):
     pts = torch.as_tensor(g["points"], device="cuda")
     v = build_table(wfn, basis, Pd, pts).esp(pts).cpu().numpy()
     np.testing.assert_allclose(v, g["esp_t12"], rtol=0, atol=1e-12)
+
+
+def test_surface_points_match_reference_sampler(golden, tmp_path):
+    """The GPU sampler in mode="reference" at 1.0x radii against the points the
+    reference's own sampler (examples/vdw_surface_esp.py:38-52) drew for the
+    same molecules and seeds (tests/golden/ref_points.npz)."""
+    from fastesp_b200 import read_molden
+    g = golden("ref_points")
+    for key in g.files:
+        tag, n, seed = key.split("_")
+        wfn = read_molden(synth.make_system(tag, 0).write(tmp_path / f"{tag}.molden"))
+        got = surface_points(wfn.symbols, wfn.coords, int(n), seed=int(seed), scale=1.0,
+                             mode="reference").cpu().numpy()
+        want = g[key]
+        assert got.shape == want.shape, key
+        assert np.abs(got - want).max() < 1e-12, key

@@ -255,3 +255,22 @@ def test_molden_reader_fast_and_fallback_paths_agree(tmp_path):
     w1 = read_molden(p)
     np.testing.assert_array_equal(w1.mo_occ, w0.mo_occ)
     np.testing.assert_allclose(w1.mo_coeff, w0.mo_coeff, rtol=1e-12, atol=0)
+
+
+def _ref_sampler_cases(golden, tmp_path):
+    from fastesp_b200 import read_molden
+    g = golden("ref_points")
+    for key in g.files:
+        tag, n, seed = key.split("_")
+        wfn = read_molden(synth.make_system(tag, 0).write(tmp_path / f"{tag}.molden"))
+        yield wfn, int(n), int(seed), g[key]
+
+
+def test_host_sampler_reproduces_reference_sampler(golden, tmp_path):
+    """mode="reference" at 1.0x radii draws the reference sampler's points
+    (examples/vdw_surface_esp.py:38-52) for the same seed, in its order."""
+    for wfn, n, seed, want in _ref_sampler_cases(golden, tmp_path):
+        got = synth.vdw_surface_points(wfn.symbols, wfn.coords, n, seed=seed, scale=1.0,
+                                       mode="reference")
+        assert got.shape == want.shape
+        np.testing.assert_allclose(got, want, rtol=0, atol=1e-12)
