@@ -46,7 +46,11 @@ def headline(frag54, tmp_path_factory):
     td = tmp_path_factory.mktemp("headline")
     bb, pb, out = td / "basis.bin", td / "pairs.bin", td / "esp.txt"
     write_basis_payload(bb, basis_payload(wfn, basis, P, pts))
-    env = dict(os.environ, OMP_NUM_THREADS=str(len(os.sched_getaffinity(0))))
+    # one thread: with OpenMP the builder appends each thread's pairs when the
+    # thread finishes (build_pairs.cpp:194-381), so only a single-threaded run
+    # has the reference's nominal pair order (shell pairs si <= sj in order,
+    # primitive of si outer), which this package's tables keep per class
+    env = dict(os.environ, OMP_NUM_THREADS="1")
     r = subprocess.run([str(BUILD_PAIRS), str(bb), str(pb), "1e-12"], capture_output=True,
                        text=True, timeout=900, env=env)
     assert r.returncode == 0, r.stderr[-2000:]
