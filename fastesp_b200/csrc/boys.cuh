@@ -58,7 +58,9 @@ FE_DEV void fe_boys_f64(const double T, double (&F)[M + 1]) {
 #pragma unroll
     for (int m = 0; m < M; ++m) F[m + 1] = fma(double(2 * m + 1), F[m], -e) * h;
   } else {
-    const int i = __double2int_rn(T * FE_BOYS_GRID_INV_H);
+    // clamped: a NaN argument (a NaN point) converts to an arbitrary integer,
+    // and a malformed table could give T < 0; both must still read in bounds
+    const int i = min(max(__double2int_rn(T * FE_BOYS_GRID_INV_H), 0), FE_BOYS_NROW - 1);
     const double d = -(T - double(i) * FE_BOYS_GRID_H);   // exact: |d| <= h/2
     const double* row = fe_boys_grid + i * FE_BOYS_NTAB + M;
     double f = __ldg(row + FE_BOYS_TAYLOR_K - 1);
@@ -111,7 +113,7 @@ FE_DEV void fe_boys_f32(const float T, const float rt, const float* __restrict__
 #pragma unroll
     for (int m = 0; m < M; ++m) F[m + 1] = (F[m] - E[m + 1]) * it;
   } else {
-    const int i = __float2int_rn(T * FE_BOYS32_GRID_INV_H);
+    const int i = min(max(__float2int_rn(T * FE_BOYS32_GRID_INV_H), 0), FE_BOYS32_NROW - 1);
     const float d = -(T - float(i) * FE_BOYS32_GRID_H);
     const float* row = grid + i * FE_BOYS32_NTAB + M;
     float f = row[FE_BOYS32_TAYLOR_K - 1];
@@ -128,26 +130,30 @@ FE_DEV void fe_boys_f32(const float T, const float rt, const float* __restrict__
   }
 }
 
-// Packed scaled FP32 Boys vectors of two arguments (one per float2 lane), for
-// the orders whose FP32 asymptotic threshold lies below the grid's end
-// (M <= 6): the tabulated and the asymptotic branch only.  Each lane gets what
-// fe_boys_f32 would give it with the scaled rows; when the lanes fall in
-// different branches both are computed and each lane keeps its own.  ``grid``
-// holds the per-order scaled rows fe_boys_grid32s (F_(M+k)/(k! s_M)), so the
-// Taylor polynomial of F^_M is evaluated in d directly.
+// Packed FP32 Boys vectors of two arguments (one per float2 lane), for the
+// orders whose FP32 asymptotic threshold lies below the grid's end (M <= 6):
+// the tabulated and the asymptotic branch only, in the form the FP32 records'
+// coefficients c_k = K G_k s_m p^-(m+1/2) take: F~_m = F_m(T) p^(m+1/2) / s_m,
+// which in the asymptotic range is exactly 1/|R|^(2m+1) (T = p |R|^2), so an
+// asymptotic lane needs only ``ir`` = 1/|R|.  A tabulated lane evaluates
+// F^_M = F_M / s_M from the per-order scaled rows fe_boys_grid32s
+// (F_(M+k)/(k! s_M), Taylor polynomial in d directly) in ``grid``, the
+// downward recursion of fe_boys_f32, then multiplies order m by
+// sqrt(p) p^m (``sp``, ``p``).  When the lanes fall in different branches both
+// are computed and each lane keeps its own.
 template <int M>
-FE_DEV void fe_boys_f32x2(const float2 T, const float2 rt, const float* __restrict__ grid,
-                          float2 (&F)[M + 1]) {
+FE_DEV void fe_boys_f32x2(const float2 T, const float2 ir, const float2 sp, const float2 p,
+                          const float* __restrict__ grid, float2 (&F)[M + 1]) {
   constexpr float t_asym = fe_boys32_asym_T[M];
   constexpr float kh = fe_boys32_kappa_hi[M], kl = fe_boys32_kappa_lo[M];
   static_assert(fe_boys32_asym_T[M] <= FE_BOYS32_GRID_TMAX, "two-branch form only");
   const bool ax = T.x >= t_asym, ay = T.y >= t_asym;
   float2 A[M + 1], G[M + 1];
   if (ax || ay) {
-    const float2 it = rt * rt;
-    A[0] = rt;
+    const float2 ir2 = ir * ir;
+    A[0] = ir;
 #pragma unroll
-    for (int m = 0; m < M; ++m) A[m + 1] = A[m] * it;
+    for (int m = 0; m < M; ++m) A[m + 1] = A[m] * ir2;
   }
   if (!(ax && ay)) {
     // a lane in the asymptotic range reads a clamped, in-range row; its result is dropped
@@ -167,6 +173,13 @@ FE_DEV void fe_boys_f32x2(const float2 T, const float2 rt, const float* __restri
     for (int m = M; m > 0; --m) {
       G[m - 1] = fe_fma(T, G[m], E);
       if (m > 1) E = E * fe_f2(float(2 * m - 1) * 0.5f);
+    }
+    float2 w = sp;
+    G[0] = G[0] * w;
+#pragma unroll
+    for (int m = 1; m <= M; ++m) {
+      w = w * p;
+      G[m] = G[m] * w;
     }
   }
   if (ax && ay) {

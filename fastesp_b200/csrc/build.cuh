@@ -530,9 +530,47 @@ __global__ void __launch_bounds__(FE_SCAN_BLOCK) fe_scan_apply_kernel(
   if (i < n) pos[i] = bsum[blockIdx.x] + buf[threadIdx.x] - v;
 }
 
-// Mixed-precision records from the FP64 records: every FP64 value as a float
-// hi/lo pair (layout in table.cuh).
-__global__ void fe_make_f32_kernel(unsigned char* table) {
+// Radius beyond which sum_n b_n / r^(n+1) < tau (b_n >= 0): with u = 1/r the
+// sum is convex and increasing in u, so Newton's method started above the root
+// (at the smallest u where one term alone reaches tau) descends to it
+// monotonically.  0 when every b_n is 0 (never routed); +inf when a b_n is not
+// finite.  Widened by 1e-6 relative so the radius is never below the exact one.
+FE_DEV double fe_route_radius(const double* b, int L, double tau) {
+  double u = 1e300;
+  bool any = false;
+  for (int n = 0; n <= L; ++n) {
+    if (!(b[n] >= 0.0) || isinf(b[n])) return __longlong_as_double(0x7ff0000000000000LL);
+    if (b[n] > 0.0) {
+      u = fmin(u, pow(tau / b[n], 1.0 / double(n + 1)));
+      any = true;
+    }
+  }
+  if (!any) return 0.0;
+  for (int it = 0; it < 100; ++it) {
+    double g = 0.0, dg = 0.0;                 // g = sum b_n u^n and g'(u), Horner
+    for (int n = L; n >= 0; --n) {
+      dg = fma(dg, u, g);
+      g = fma(g, u, b[n]);
+    }
+    const double f = u * g, df = fma(u, dg, g);   // f = u g, f' = g + u g'
+    const double step = (f - tau) / df;
+    if (!(step > 1e-15 * u)) break;
+    u -= step;
+  }
+  return (1.0 + 1e-6) / u;
+}
+
+// FP32 asymptotic Boys thresholds by class, for runtime indexing.
+__constant__ float fe_c_boys32_asym_T[FE_NCLASS] = {
+  fe_boys32_asym_T[0], fe_boys32_asym_T[1], fe_boys32_asym_T[2], fe_boys32_asym_T[3],
+  fe_boys32_asym_T[4], fe_boys32_asym_T[5], fe_boys32_asym_T[6], fe_boys32_asym_T[7],
+  fe_boys32_asym_T[8]};
+
+// Mixed-precision records from the FP64 records (layout in table.cuh):
+// coefficients c_k = K G_k s_m p^-(m+1/2) and the routing-bound coefficients
+// formed in FP64, then rounded to float once.  ``tau_fast`` is the routing
+// threshold the far radius is computed for.
+__global__ void fe_make_f32_kernel(unsigned char* table, float tau_fast) {
   FeTableHdr* hdr = reinterpret_cast<FeTableHdr*>(table);
   const int L = blockIdx.y;
   const int n = hdr->count[L];
@@ -546,32 +584,50 @@ __global__ void fe_make_f32_kernel(unsigned char* table) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double* r = src + size_t(i) * R64;
     float* o = dst + size_t(i) * R32;
-    split(r[0], o[0], o[1]);
+    const double p = r[0], K = r[4];
+    o[0] = float(p);
+    o[1] = float(sqrt(p));
 #pragma unroll
     for (int k = 0; k < 3; ++k) split(r[1 + k], o[2 + k], o[5 + k]);
-    split(r[4], o[8], o[9]);
-    o[10] = float(r[5]);                 // K * bound (+inf when unknown)
-    o[11] = float(1.0 / sqrt(r[0]));     // p^-1/2
-    // coefficients times s_m = (sqrt(pi)/2) (2m-1)!!/2^m, in FP64: the FP32
-    // evaluator's Boys vector is F_m / s_m (boys.cuh)
-    double sm[FE_NCLASS];
+    o[9] = float(1.0 / sqrt(p));
+    o[10] = o[11] = 0.0f;
+    // s_m = (sqrt(pi)/2) (2m-1)!!/2^m (the FP32 Boys vector is F_m / s_m,
+    // boys.cuh) and p^-(m+1/2): with both folded in, F_m of an asymptotic
+    // point is 1/|R|^(2m+1) exactly
+    double sm[FE_NCLASS], pm[FE_NCLASS];
     sm[0] = FE_SQRT_PI_2;
-    for (int m = 1; m <= L; ++m) sm[m] = sm[m - 1] * (0.5 * double(2 * m - 1));
+    pm[0] = 1.0 / sqrt(p);
+    for (int m = 1; m <= L; ++m) {
+      sm[m] = sm[m - 1] * (0.5 * double(2 * m - 1));
+      pm[m] = pm[m - 1] / p;
+    }
     const int c0 = fe_route_off[L];
-    for (int k = 0; k < NT; ++k)
-      o[12 + 2 * k] = o[13 + 2 * k] = float(r[6 + k] * sm[fe_route_nm[c0 + k] >> 4]);
+    for (int k = 0; k < NT; ++k) {
+      const int m = fe_route_nm[c0 + k] >> 4;
+      o[12 + 2 * k] = o[13 + 2 * k] = float(K * r[6 + k] * sm[m] * pm[m]);
+    }
     // routing bound: K sum_k |G_k R^a F_m| <= sum_n b_n / |R|^(n+1) with
     // b_n = K sum_{k: 2m - |a| = n} |G_k| c_k p^-(m + 1/2); rounded up to float
-    double b[FE_NCLASS], pm[FE_NCLASS];
-    pm[0] = 1.0 / sqrt(r[0]);
-    for (int m = 1; m <= L; ++m) pm[m] = pm[m - 1] / r[0];
-    for (int n = 0; n <= L; ++n) b[n] = 0.0;
+    double b[FE_NCLASS];
+    for (int q = 0; q <= L; ++q) b[q] = 0.0;
     for (int k = 0; k < NT; ++k) {
       const unsigned nm = fe_route_nm[c0 + k];
       b[nm & 15u] += fabs(r[6 + k]) * fe_route_c[c0 + k] * pm[nm >> 4];
     }
-    for (int n = 0; n <= L; ++n) o[12 + 2 * NT + n] = __double2float_ru(r[4] * b[n]);
+    for (int q = 0; q <= L; ++q) {
+      o[12 + 2 * NT + q] = __double2float_ru(K * b[q]);
+      b[q] = double(o[12 + 2 * NT + q]);
+    }
+    // far radius: the FP32 Boys vector is asymptotic (T = p r^2 beyond the
+    // class's FP32 threshold) and the bound (with the stored, rounded-up b_n)
+    // is below tau_fast
+    const double rt = fe_route_radius(b, L, double(tau_fast));
+    const double ra2 = double(fe_c_boys32_asym_T[L]) / p * (1.0 + 1e-6);
+    o[8] = __double2float_ru(fmax(ra2, rt * rt));
     for (int k = 13 + 2 * NT + L; k < R32; ++k) o[k] = 0.0f;
   }
-  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) hdr->has32 = 1;
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+    hdr->has32 = 1;
+    hdr->tau_fast = tau_fast;
+  }
 }

@@ -108,6 +108,8 @@ FE_DEV void fe_load_points_split(const double* __restrict__ pts, int npts, int p
 // mask instead.  ``first`` is the class-local index of the tile's first pair,
 // ``hi`` the end of this split's range of the class; ``bits`` carries the
 // current mask word across tiles (identical in every lane, lane 0 stores it).
+// The record's coefficients carry K and p^-(m+1/2) (table.cuh), so the scaled
+// Boys vector F^_m of fe_boys_f32 is multiplied by sqrt(p) p^m.
 template <int L, int NP>
 FE_DEV void fe_tile_f32(const float* __restrict__ rec, int first, int n, int hi,
                         const float (&cxh)[NP], const float (&cyh)[NP], const float (&czh)[NP],
@@ -127,37 +129,34 @@ FE_DEV void fe_tile_f32(const float* __restrict__ rec, int first, int n, int hi,
       bits = 0u;
     }
     if (routed) continue;
-    const float pe = rec[0], rsp = rec[11], K = rec[8];
+    const float pe = rec[0], sp = rec[1], rsp = rec[9];
     float F[NP][L + 1], s[NP];
 #pragma unroll
-    for (int j = 0; j < NP; ++j) fe_boys_f32<L>(pe * r2[j], ir[j] * rsp, grid, F[j]);
+    for (int j = 0; j < NP; ++j) {
+      fe_boys_f32<L>(pe * r2[j], ir[j] * rsp, grid, F[j]);
+      float w = sp;
+      F[j][0] *= w;
+#pragma unroll
+      for (int m = 1; m <= L; ++m) {
+        w *= pe;
+        F[j][m] *= w;
+      }
+    }
     fe_poly<L, float, NP>(rec + 12, x, y, z, F, s);
 #pragma unroll
-    for (int j = 0; j < NP; ++j) acc[j] += double(K * s[j]);
+    for (int j = 0; j < NP; ++j) acc[j] += double(s[j]);
   }
 }
 
-// The same routing test and FP32 evaluation with two points per float2 lane
-// (packed FP32x2 instructions; point 2q + e of the thread in lane e of q).
-// Lane by lane the routing test is that of fe_route; the Boys vector comes
-// from the per-order scaled rows (fe_boys_f32x2).
+// The routing test of fe_route for two points per float2 lane, from |R|^2:
+// also returns ir = 1/|R|.
 template <int L, int NQ>
-FE_DEV bool fe_route2(const float* __restrict__ rec, const float2 (&cxh)[NQ],
-                      const float2 (&cyh)[NQ], const float2 (&czh)[NQ], const float2 (&cxl)[NQ],
-                      const float2 (&cyl)[NQ], const float2 (&czl)[NQ], float2 (&x)[NQ],
-                      float2 (&y)[NQ], float2 (&z)[NQ], float2 (&r2)[NQ], float2 (&ir)[NQ],
+FE_DEV bool fe_route2(const float* __restrict__ rec, const float2 (&r2)[NQ], float2 (&ir)[NQ],
                       float tau) {
-  // fe_route for two points per lane: bound sum_n b_n / |R|^(n+1) in Horner form in 1/|R|
   const float* bn = rec + 12 + 2 * fe_class_nterm[L];
-  const float2 pxh = fe_f2(rec[2]), pyh = fe_f2(rec[3]), pzh = fe_f2(rec[4]);
-  const float2 pxl = fe_f2(rec[5]), pyl = fe_f2(rec[6]), pzl = fe_f2(rec[7]);
   bool need = false;
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
-    x[q] = (cxh[q] - pxh) + (cxl[q] - pxl);
-    y[q] = (cyh[q] - pyh) + (cyl[q] - pyl);
-    z[q] = (czh[q] - pzh) + (czl[q] - pzl);
-    r2[q] = fe_fma(x[q], x[q], fe_fma(y[q], y[q], z[q] * z[q]));
     ir[q] = make_float2(rsqrtf(r2[q].x), rsqrtf(r2[q].y));
     float2 bound = fe_f2(bn[L]);
 #pragma unroll
@@ -168,36 +167,76 @@ FE_DEV bool fe_route2(const float* __restrict__ rec, const float2 (&cxh)[NQ],
   return __any_sync(0xffffffffu, need);
 }
 
+// The same with two points per float2 lane (packed FP32x2 instructions; point
+// 2q + e of the thread in lane e of q).  Per pair, R and |R|^2 first; then
+//  * far pairs -- every point of the warp at least the record's rfar from the
+//    centre (only when ``fast``: the routing threshold is at least the one rfar
+//    was computed for): no point routes and every Boys vector is asymptotic,
+//    F~_m = 1/|R|^(2m+1), so s = (1/|R|) sum_m (1/|R|^2)^m h_m (fe_poly32x2a);
+//  * the others: the exact per-point routing test of fe_route, then the Boys
+//    vectors of fe_boys_f32x2 and the polynomial.
+// The far test is a sufficient condition for the others' outcome (no route,
+// asymptotic branch), so both give the same decisions; it only skips work.
 template <int L, int NQ>
 FE_DEV void fe_tile_f32x2(const float* __restrict__ rec, int first, int n, int hi,
                           const float2 (&cxh)[NQ], const float2 (&cyh)[NQ],
                           const float2 (&czh)[NQ], const float2 (&cxl)[NQ],
                           const float2 (&cyl)[NQ], const float2 (&czl)[NQ],
                           double (&acc)[2 * NQ], const float* __restrict__ grid, float tau,
-                          unsigned* __restrict__ mw, unsigned& bits) {
+                          bool fast, unsigned* __restrict__ mw, unsigned& bits) {
   constexpr int S32 = fe_class_rec32[L];
   const bool lane0 = (threadIdx.x & 31) == 0;
 #pragma unroll 1
   for (int i = 0; i < n; ++i, rec += S32) {
     const int gi = first + i;
-    float2 x[NQ], y[NQ], z[NQ], r2[NQ], ir[NQ];
-    const bool routed = fe_route2<L, NQ>(rec, cxh, cyh, czh, cxl, cyl, czl, x, y, z, r2, ir, tau);
+    const float2 pxh = fe_f2(rec[2]), pyh = fe_f2(rec[3]), pzh = fe_f2(rec[4]);
+    const float2 pxl = fe_f2(rec[5]), pyl = fe_f2(rec[6]), pzl = fe_f2(rec[7]);
+    const float rf2 = rec[8];
+    float2 x[NQ], y[NQ], z[NQ], r2[NQ];
+    bool far = fast;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      x[q] = (cxh[q] - pxh) + (cxl[q] - pxl);
+      y[q] = (cyh[q] - pyh) + (cyl[q] - pyl);
+      z[q] = (czh[q] - pzh) + (czl[q] - pzl);
+      r2[q] = fe_fma(x[q], x[q], fe_fma(y[q], y[q], z[q] * z[q]));
+      far = far && r2[q].x >= rf2 && r2[q].y >= rf2;
+    }
+    bool routed = false;
+    if (__all_sync(0xffffffffu, far)) {
+      float2 ir[NQ], ir2[NQ], s[NQ];
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        ir[q] = make_float2(rsqrtf(r2[q].x), rsqrtf(r2[q].y));
+        ir2[q] = ir[q] * ir[q];
+      }
+      fe_poly32x2a<L, NQ>(rec + 12, x, y, z, ir2, s);
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        const float2 v = s[q] * ir[q];
+        acc[2 * q] += double(v.x);
+        acc[2 * q + 1] += double(v.y);
+      }
+    } else {
+      float2 ir[NQ];
+      routed = fe_route2<L, NQ>(rec, r2, ir, tau);
+      if (!routed) {
+        const float2 pe = fe_f2(rec[0]), sp = fe_f2(rec[1]);
+        float2 F[NQ][L + 1], s[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) fe_boys_f32x2<L>(pe * r2[q], ir[q], sp, pe, grid, F[q]);
+        fe_poly32x2<L, NQ>(rec + 12, x, y, z, F, s);
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+          acc[2 * q] += double(s[q].x);
+          acc[2 * q + 1] += double(s[q].y);
+        }
+      }
+    }
     bits |= unsigned(routed) << (gi & 31);
     if ((gi & 31) == 31 || gi + 1 == hi) {
       if (lane0 && mw) mw[gi >> 5] = bits;
       bits = 0u;
-    }
-    if (routed) continue;
-    const float2 pe = fe_f2(rec[0]), rsp = fe_f2(rec[11]), K = fe_f2(rec[8]);
-    float2 F[NQ][L + 1], s[NQ];
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) fe_boys_f32x2<L>(pe * r2[q], ir[q] * rsp, grid, F[q]);
-    fe_poly32x2<L, NQ>(rec + 12, x, y, z, F, s);
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) {
-      const float2 v = K * s[q];
-      acc[2 * q] += double(v.x);
-      acc[2 * q + 1] += double(v.y);
     }
   }
 }
@@ -286,6 +325,8 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
     fe_flag(FE_ST_OVERFLOW);
   }
   unsigned bits = 0u;
+  // the records' far radius holds for routing thresholds at least tau_fast
+  const bool fast = a.tau >= hdr->tau_fast;
   for (int i = 0; i < total; ++i) {
     if (!pipe.wait(i)) {
       pipe.abort(i);
@@ -298,7 +339,7 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
     unsigned* mw = mrow ? mrow + w.woff[L] : nullptr;
     if constexpr (PACKED) {
 #define FE_CALL32(l) fe_tile_f32x2<l, NQ>(rec, first, n, w.hi[L], cxh2, cyh2, czh2, cxl2, cyl2, \
-                                          czl2, acc, grid, a.tau, mw, bits)
+                                          czl2, acc, grid, a.tau, fast, mw, bits)
       FE_MX_SWITCH(FE_CALL32)
 #undef FE_CALL32
     } else {

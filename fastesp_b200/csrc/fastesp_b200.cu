@@ -54,6 +54,14 @@ int fail(int code, const char* fmt, ...) {
 
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Default FP64 routing threshold of the mixed evaluator (a.u.): the largest
+// setting that kept the error against the FP64 path below 1e-6 a.u., with a
+// margin, on the 54-atom l<=3 system (three 30000-point surface samples and the
+// 568,950-point cubic grid, worst 7.7e-7; 0.05 reached 1.02e-6 on the grid).
+// The FP32 records' far radius is computed for it, so smaller thresholds
+// evaluate every pair through the exact per-point routing test.
+constexpr double kTauDefault = 0.04;
+
 int sm_count() {
   int dev = 0, n = 148;
   if (cudaGetDevice(&dev) == cudaSuccess)
@@ -489,7 +497,8 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
   }
   fe_finalize_kernel<<<1, 1024, 0, st>>>(a.class_slot0, FE_NCLASS, p->nslot, a.keep, pos, a.srule, tb);
   FE_CUDA(cudaGetLastError());
-  fe_make_f32_kernel<<<dim3(std::max(1, 2 * sm_count() / FE_NCLASS), FE_NCLASS), 256, 0, st>>>(tb);
+  fe_make_f32_kernel<<<dim3(std::max(1, 2 * sm_count() / FE_NCLASS), FE_NCLASS), 256, 0, st>>>(
+      tb, float(kTauDefault));
   FE_CUDA(cudaGetLastError());
   return FE_OK;
 }
@@ -530,7 +539,7 @@ int fe_table_init(void* d_table, const int* count, int n_atoms, const double* Z,
 int fe_table_make_f32(void* d_table, cudaStream_t st) {
   if (!d_table) return fail(FE_ERR_ARG, "fe_table_make_f32: null table");
   fe_make_f32_kernel<<<dim3(std::max(1, 2 * sm_count() / FE_NCLASS), FE_NCLASS), 256, 0, st>>>(
-      static_cast<unsigned char*>(d_table));
+      static_cast<unsigned char*>(d_table), float(kTauDefault));
   FE_CUDA(cudaGetLastError());
   return FE_OK;
 }
@@ -648,12 +657,6 @@ int eval_launch(const char* who, const void* d_table, const double* d_pts, int n
   FE_CUDA(cudaGetLastError());
   return FE_OK;
 }
-
-// Default FP64 routing threshold of the mixed evaluator (a.u.): the largest
-// setting that kept the error against the FP64 path below 1e-6 a.u., with a
-// margin, on the 54-atom l<=3 system (three 30000-point surface samples and the
-// 568,950-point cubic grid, worst 7.7e-7; 0.05 reached 1.02e-6 on the grid).
-constexpr double kTauDefault = 0.04;
 
 }  // namespace
 

@@ -137,7 +137,13 @@ class CoefLoader:
         return [k for k, _ in sorted(self.pos.items(), key=lambda kv: kv[1])]
 
 
-def poly_m_major(L, order=None, vec=0, vtype="", dup=None):
+def poly_m_major(L, order=None, vec=0, vtype="", dup=None, asym=False):
+    """s = sum_m F_m h_m(R), h_m the Horner polynomial of the order-m terms,
+    orders taken from the highest down (the coefficient consumption order).
+
+    ``asym``: the form for points where every F_m is asymptotic and the
+    coefficients carry p^-(m+1/2), so F_m is 1/|R|^(2m+1): s = sum_m ir2^m
+    h_m, in Horner form in ir2 = 1/|R|^2 (the caller multiplies by 1/|R|)."""
     keys, _ = H.class_terms(L)
     em = Emitter()
     ld = CoefLoader(em, order, vec, vtype, dup)
@@ -145,15 +151,29 @@ def poly_m_major(L, order=None, vec=0, vtype="", dup=None):
     for k, (ax, ay, az, m) in enumerate(keys):
         by_m.setdefault(m, {})[(ax, ay, az)] = k
     acc = ("ha", "hb", "hc")
-    first = True
-    for m in sorted(by_m):
+    prev = None
+    for m in sorted(by_m, reverse=True):
         em.horner(by_m[m], 0, acc, lambda k: (None, ld.expr(k)))
-        if first:
+        if asym:
+            if prev is None:
+                em.w("FE_UNROLL for (int j = 0; j < NP; ++j) s[j] = ha[j];")
+            else:
+                for _ in range(prev - m - 1):
+                    em.w("FE_UNROLL for (int j = 0; j < NP; ++j) s[j] *= ir2[j];")
+                    em.nops += 1
+                em.w("FE_UNROLL for (int j = 0; j < NP; ++j) s[j] = fe_fma(s[j], ir2[j], ha[j]);")
+                em.nops += 1
+        elif prev is None:
             em.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) s[j] = F[j][{m}] * ha[j];")
-            first = False
+            em.nops += 1
         else:
             em.w(f"FE_UNROLL for (int j = 0; j < NP; ++j) s[j] = fe_fma(F[j][{m}], ha[j], s[j]);")
-        em.nops += 1
+            em.nops += 1
+        prev = m
+    if asym:
+        for _ in range(prev):
+            em.w("FE_UNROLL for (int j = 0; j < NP; ++j) s[j] *= ir2[j];")
+            em.nops += 1
     return em, ld
 
 
@@ -229,7 +249,7 @@ def poly_functions(L):
                                           ("float2", "float4", 4, "32x2", "packed"),
                                           ("double", "double2", 2, "64", None)):
         em, _ = build(L, order, vec, vtype, dup)
-        lay = ("coefficients g[2k] = g[2k+1] = G_k in consumption order" if dup else
+        lay = ("coefficients g[2k] = g[2k+1] = c_k in consumption order" if dup else
                "coefficients g[k] in consumption order")
         out += [f"// class L={L}: {H.n_terms(L)} terms, {nops} fused ops per point ({tag}),",
                 f"// {lay}, 16-byte aligned"
@@ -241,6 +261,22 @@ def poly_functions(L):
                 "  using Real = " + real + ";",
                 "  Real ha[NP], hb[NP], hc[NP], hd[NP];",
                 "  (void)hb; (void)hc; (void)hd;"]
+        out += em.lines
+        out.append("}")
+        out.append("")
+    if tag == "m-major":
+        # the asymptotic form of the packed FP32 code (see poly_m_major)
+        em, _ = poly_m_major(L, order, 4, "float4", "packed", asym=True)
+        out += [f"// class L={L}: the packed form for points whose Boys vectors are all",
+                "// asymptotic: s = sum_m ir2^m h_m (Horner in ir2 = 1/|R|^2); the caller",
+                "// multiplies by 1/|R|; coefficients as fe_poly32x2_L" + str(L),
+                "template <int NP>",
+                f"__device__ __forceinline__ void fe_poly32x2a_L{L}(const float* __restrict__ g,",
+                "    const float2 (&x)[NP], const float2 (&y)[NP], const float2 (&z)[NP],",
+                "    const float2 (&ir2)[NP], float2 (&s)[NP]) {",
+                "  using Real = float2;",
+                "  Real ha[NP], hb[NP], hc[NP], hd[NP];",
+                "  (void)hb; (void)hc; (void)hd; (void)ir2;"]
         out += em.lines
         out.append("}")
         out.append("")
@@ -601,6 +637,18 @@ def main() -> int:
     for L in range(LMAX + 1):
         kw = "if" if L == 0 else "else if"
         out.append(f"  {kw} constexpr (L == {L}) fe_poly32x2_L{L}<NP>(g, x, y, z, F, s);")
+    out.append("}")
+    out.append("")
+    out.append("// the asymptotic packed form (m-major classes only)")
+    out.append("template <int L, int NP>")
+    out.append("__device__ __forceinline__ void fe_poly32x2a(const float* __restrict__ g,")
+    out.append("    const float2 (&x)[NP], const float2 (&y)[NP], const float2 (&z)[NP],")
+    out.append("    const float2 (&ir2)[NP], float2 (&s)[NP]) {")
+    for L in range(LMAX + 1):
+        if poly_variant(L)[1] != "m-major":
+            continue
+        kw = "if" if L == 0 else "else if"
+        out.append(f"  {kw} constexpr (L == {L}) fe_poly32x2a_L{L}<NP>(g, x, y, z, ir2, s);")
     out.append("}")
     out.append("")
     out.append("template <int L, typename Real, int NP>")

@@ -15,14 +15,17 @@
 // the reference builder: shell pairs (si <= sj) in shell order, then
 // primitive pairs with the primitive of shell si outer.
 //
-// Mixed-precision records are fe_class_rec32[L] floats: the pair's scalars as
+// Mixed-precision records are fe_class_rec32[L] floats: the pair's centre as
 // hi = float(v), lo = float(v - hi) splits, then every coefficient twice, so
-// a 16-byte load yields two coefficients each already a {g, g} operand pair
+// a 16-byte load yields two coefficients each already a {c, c} operand pair
 // of the packed FP32x2 arithmetic:
-// [p_hi, p_lo, Px_hi, Py_hi, Pz_hi, Px_lo, Py_lo, Pz_lo, K_hi, K_lo, K*bound,
-//  p^-1/2, G_0, G_0, G_1, G_1, ..., G_(nt-1), G_(nt-1), b_0, .., b_L, pad to
-//  16 bytes] (G in the same consumption order as the FP64 record; b_n the
-// coefficients of the routing bound sum_n b_n / |R|^(n+1), eval_mixed.cuh).
+// [p, sqrt(p), Px_hi, Py_hi, Pz_hi, Px_lo, Py_lo, Pz_lo, rfar^2, p^-1/2, 0, 0,
+//  c_0, c_0, c_1, c_1, ..., c_(nt-1), c_(nt-1), b_0, .., b_L, pad to 16 bytes]
+// with c_k = K G_k s_m p^-(m+1/2) formed in FP64 (s_m the Boys scale factor,
+// boys.cuh), in the same consumption order as the FP64 record's G; b_n the
+// coefficients of the routing bound sum_n b_n / |R|^(n+1); rfar the radius
+// beyond which the pair's FP32 Boys vector is asymptotic and the routing
+// bound is below the header's tau_fast (eval_mixed.cuh).
 //
 // The source section maps every record of a table built on the device back to
 // the builder's work item (shell pair and primitive indices), so the adjoint
@@ -50,6 +53,8 @@ struct FeTableHdr {
   int32_t has32;                     // FP32 records are current
   int32_t has_src;                   // the source section is filled
   int64_t off_src;                   // byte offset of the source section
+  float tau_fast;                    // routing threshold of the FP32 records' far radius
+  int32_t pad_;
 };
 
 static_assert(sizeof(FeTableHdr) <= 512, "header must fit its slot");

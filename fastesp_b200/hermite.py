@@ -105,11 +105,12 @@ def record_stride(L: int) -> int:
 def record_stride_f32(L: int) -> int:
     """FP32 words per mixed-precision record, padded to 16 bytes.
 
-    The pair's scalars as float pairs hi = float(v), lo = float(v - hi), then
-    every coefficient twice (a {g, g} operand pair of the packed FP32x2 code),
-    then the L + 1 coefficients of the routing bound sum_n b_n / |R|^(n+1):
-    [p_hi, p_lo, Px_hi, Py_hi, Pz_hi, Px_lo, Py_lo, Pz_lo, K_hi, K_lo, K*bound,
-    p^-1/2, G_0, G_0, G_1, G_1, ..., b_0, .., b_L].
+    The pair's scalars (the centre as float pairs hi = float(v), lo =
+    float(v - hi)), then every coefficient twice (a {c, c} operand pair of the
+    packed FP32x2 code), then the L + 1 coefficients of the routing bound
+    sum_n b_n / |R|^(n+1): [p, sqrt(p), Px_hi, Py_hi, Pz_hi, Px_lo, Py_lo,
+    Pz_lo, rfar^2, p^-1/2, 0, 0, c_0, c_0, c_1, c_1, ..., b_0, .., b_L] with
+    c_k = K G_k s_m p^-(m+1/2) (csrc/table.cuh).
     """
     n = 12 + 2 * n_terms(L) + L + 1
     return (n + 3) // 4 * 4
