@@ -186,56 +186,64 @@ FE_DEV void fe_tile_f32x2(const float* __restrict__ rec, int first, int n, int h
                           bool fast, unsigned* __restrict__ mw, unsigned& bits) {
   constexpr int S32 = fe_class_rec32[L];
   const bool lane0 = (threadIdx.x & 31) == 0;
+  // pairs in runs that end on a routing-mask word boundary (or the split's
+  // end), so the word is stored once per run, not tested per pair
+  for (int i = 0; i < n;) {
+    const int gi0 = first + i;
+    const int run = min(n - i, 32 - (gi0 & 31));
 #pragma unroll 1
-  for (int i = 0; i < n; ++i, rec += S32) {
-    const int gi = first + i;
-    const float2 pxh = fe_f2(rec[2]), pyh = fe_f2(rec[3]), pzh = fe_f2(rec[4]);
-    const float2 pxl = fe_f2(rec[5]), pyl = fe_f2(rec[6]), pzl = fe_f2(rec[7]);
-    const float rf2 = rec[8];
-    float2 x[NQ], y[NQ], z[NQ], r2[NQ];
-    bool far = fast;
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) {
-      x[q] = (cxh[q] - pxh) + (cxl[q] - pxl);
-      y[q] = (cyh[q] - pyh) + (cyl[q] - pyl);
-      z[q] = (czh[q] - pzh) + (czl[q] - pzl);
-      r2[q] = fe_fma(x[q], x[q], fe_fma(y[q], y[q], z[q] * z[q]));
-      far = far && r2[q].x >= rf2 && r2[q].y >= rf2;
-    }
-    bool routed = false;
-    if (__all_sync(0xffffffffu, far)) {
-      float2 ir[NQ], ir2[NQ], s[NQ];
+    for (int r = 0; r < run; ++r, rec += S32) {
+      const float4 h0 = *reinterpret_cast<const float4*>(rec);
+      const float4 h1 = *reinterpret_cast<const float4*>(rec + 4);
+      const float rf2 = rec[8];
+      const float2 pxh = fe_f2(h0.z), pyh = fe_f2(h0.w), pzh = fe_f2(h1.x);
+      const float2 pxl = fe_f2(h1.y), pyl = fe_f2(h1.z), pzl = fe_f2(h1.w);
+      float2 x[NQ], y[NQ], z[NQ], r2[NQ];
+      bool far = fast;
 #pragma unroll
       for (int q = 0; q < NQ; ++q) {
-        ir[q] = make_float2(rsqrtf(r2[q].x), rsqrtf(r2[q].y));
-        ir2[q] = ir[q] * ir[q];
+        x[q] = (cxh[q] - pxh) + (cxl[q] - pxl);
+        y[q] = (cyh[q] - pyh) + (cyl[q] - pyl);
+        z[q] = (czh[q] - pzh) + (czl[q] - pzl);
+        r2[q] = fe_fma(x[q], x[q], fe_fma(y[q], y[q], z[q] * z[q]));
+        far = far && r2[q].x >= rf2 && r2[q].y >= rf2;
       }
-      fe_poly32x2a<L, NQ>(rec + 12, x, y, z, ir2, s);
-#pragma unroll
-      for (int q = 0; q < NQ; ++q) {
-        const float2 v = s[q] * ir[q];
-        acc[2 * q] += double(v.x);
-        acc[2 * q + 1] += double(v.y);
-      }
-    } else {
-      float2 ir[NQ];
-      routed = fe_route2<L, NQ>(rec, r2, ir, tau);
-      if (!routed) {
-        const float2 pe = fe_f2(rec[0]), sp = fe_f2(rec[1]);
-        float2 F[NQ][L + 1], s[NQ];
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) fe_boys_f32x2<L>(pe * r2[q], ir[q], sp, pe, grid, F[q]);
-        fe_poly32x2<L, NQ>(rec + 12, x, y, z, F, s);
+      if (__all_sync(0xffffffffu, far)) {
+        float2 ir[NQ], ir2[NQ], s[NQ];
 #pragma unroll
         for (int q = 0; q < NQ; ++q) {
-          acc[2 * q] += double(s[q].x);
-          acc[2 * q + 1] += double(s[q].y);
+          ir[q] = make_float2(rsqrtf(r2[q].x), rsqrtf(r2[q].y));
+          ir2[q] = ir[q] * ir[q];
+        }
+        fe_poly32x2a<L, NQ>(rec + 12, x, y, z, ir2, s);
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+          const float2 v = s[q] * ir[q];
+          acc[2 * q] += double(v.x);
+          acc[2 * q + 1] += double(v.y);
+        }
+      } else {
+        float2 ir[NQ];
+        if (fe_route2<L, NQ>(rec, r2, ir, tau)) {
+          bits |= 1u << ((gi0 + r) & 31);
+        } else {
+          const float2 pe = fe_f2(h0.x), sp = fe_f2(h0.y);
+          float2 F[NQ][L + 1], s[NQ];
+#pragma unroll
+          for (int q = 0; q < NQ; ++q) fe_boys_f32x2<L>(pe * r2[q], ir[q], sp, pe, grid, F[q]);
+          fe_poly32x2<L, NQ>(rec + 12, x, y, z, F, s);
+#pragma unroll
+          for (int q = 0; q < NQ; ++q) {
+            acc[2 * q] += double(s[q].x);
+            acc[2 * q + 1] += double(s[q].y);
+          }
         }
       }
     }
-    bits |= unsigned(routed) << (gi & 31);
-    if ((gi & 31) == 31 || gi + 1 == hi) {
-      if (lane0 && mw) mw[gi >> 5] = bits;
+    i += run;
+    const int gl = first + i - 1;                  // last pair of the run
+    if ((gl & 31) == 31 || gl + 1 == hi) {
+      if (lane0 && mw) mw[gl >> 5] = bits;
       bits = 0u;
     }
   }

@@ -318,8 +318,17 @@ int fe_plan_create(const fe_basis* b, fe_plan** out) {
     so += cls_count[L] * fe_class_rec64[L];
   }
   p->nslot = p->class_slot0[FE_NCLASS];
+  // groups heaviest first (the per-pair work grows steeply with la + lb), so the
+  // long-running blocks start in the first wave and light ones fill the tail
+  std::array<int, 25> order{};
+  for (int c = 0; c < 25; ++c) order[c] = c;
+  auto cost = [](int code) {
+    const int la = code / 5, lb = code % 5, L = la + lb;
+    return (la + 1) * (la + 2) * (lb + 1) * (lb + 2) * (L + 1) * (L + 1) * (L + 1);
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
   int block = 0;
-  for (int code = 0; code < 25; ++code) {
+  for (int code : order) {
     if (grp_tasks[code].empty()) continue;
     const int w0 = int(p->work_task.size());
     for (int ti : grp_tasks[code]) {
