@@ -510,7 +510,10 @@ def run_extras(args, dev, flush, which=("grid", "adjoint", "batch")):
                         "batched_graph_ms": tbat, "separate_launches_ms": tsep,
                         "speedup": tsep / tbat, "points_per_s": npts / (tbat * 1e-3),
                         "shape": list(b.shape), "items": b.n_items, "max_abs_diff": err,
-                        "autotune_ms": {f"{k[0]}x{k[1]}": v for k, v in (b.tuning or {}).items()}}
+                        "autotune_ms": {f"np{k[0]}_w{k[1]}_tile{k[2] // 1024}K": v
+                                        for k, v in (b.tuning or {}).items()},
+                        "shape_fields": "points per thread, work items per resident block, "
+                                        "pair-tile bytes per stage"}
     return out
 
 

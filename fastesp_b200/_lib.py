@@ -53,7 +53,7 @@ class FeBatchMol(C.Structure):
 
 
 class FeBatchShape(C.Structure):
-    _fields_ = [("points_per_thread", C.c_int), ("waves", C.c_int)]
+    _fields_ = [("points_per_thread", C.c_int), ("waves", C.c_int), ("stage_bytes", C.c_int)]
 
 
 _P = C.c_void_p

@@ -10,9 +10,11 @@ from a global queue ordered largest first; every item writes its own row of
 partial sums and a reduction adds each molecule's rows in a fixed order, so the
 values are deterministic and equal ``table.esp(points)`` to rounding of the
 split sums.  The tile shape -- points per thread (point block of 128 or 256
-points) and work items per resident block (the pair-split granularity) -- is
-picked by timing the candidates on the batch itself; the choice is cached per
-device and batch signature for the life of the process.
+points), work items per resident block (the pair-split granularity) and the
+pair tile (bytes per shared-memory stage: 8, 16 or 32 KB, i.e. how many pairs
+of a class one bulk copy brings in) -- is picked by timing the candidates on the
+batch itself; the choice is cached per device and batch signature for the life
+of the process.
 """
 from __future__ import annotations
 
@@ -21,8 +23,9 @@ import ctypes as C
 from . import _lib
 from .table import PairTable, _empty_bytes, _to_dev
 
-SHAPES = [(np_, w) for np_ in (1, 2) for w in (2, 4, 8, 16, 32)]
-DEFAULT_SHAPE = (2, 4)
+SHAPES = [(np_, w, st) for np_ in (1, 2) for w in (4, 8, 16, 32)
+          for st in (8192, 16384, 32768)]
+DEFAULT_SHAPE = (2, 4, 16384)
 _TUNED: dict = {}
 
 
@@ -60,7 +63,7 @@ class _Native:
 class BatchESP:
     """V = nuclear - electron for every (table, points) pair of a batch, FP64.
 
-    ``shape``: (points_per_thread, waves) or None to autotune.  ``graph``:
+    ``shape``: (points_per_thread, waves[, stage_bytes]) or None to autotune.  ``graph``:
     capture the launch sequence in a CUDA graph and replay it on ``run``.
     """
 
@@ -88,7 +91,7 @@ class BatchESP:
                 self.tuning = None
         else:
             self.tuning = None
-        self.shape = tuple(shape)
+        self.shape = tuple(shape) if len(shape) == 3 else tuple(shape) + (16384,)
         self._native = _Native(self._mols, self.shape, self.device)
         self._graph = None
         if graph:

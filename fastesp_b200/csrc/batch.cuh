@@ -43,7 +43,9 @@ struct FeBatchItem {
   int mol, pblock, cls, part;
 };
 
-template <int NP, int MINB, int LLO, int LHI, int Q>
+// STAGE: bytes per ring stage, i.e. the pair-tile size (STAGE / record bytes
+// pairs of a class per tile); the autotuner picks it with the point block.
+template <int NP, int MINB, int LLO, int LHI, int Q, int STAGE>
 __global__ void __launch_bounds__(128, MINB) fe_batch_f64_kernel(const unsigned char* __restrict__ desc,
                                                                  unsigned* counter,
                                                                  double* partial) {
@@ -52,12 +54,15 @@ __global__ void __launch_bounds__(128, MINB) fe_batch_f64_kernel(const unsigned 
   __shared__ uint64_t full_bar[FE_NSTAGE];
   __shared__ FeBlockWork w;
   __shared__ int item_s;
+  __shared__ int tile_s[FE_NCLASS];
+  if (threadIdx.x < FE_NCLASS) tile_s[threadIdx.x] = STAGE / (8 * fe_c_rec64[threadIdx.x]);
   const FeBatchHdr* bh = reinterpret_cast<const FeBatchHdr*>(desc);
   const FeBatchMolDev* mols = reinterpret_cast<const FeBatchMolDev*>(desc + bh->off_mol);
   const FeBatchItem* items = reinterpret_cast<const FeBatchItem*>(desc + bh->off_item[Q]);
   const int n_item = bh->n_item[Q];
   const int tid = threadIdx.x;
-  FeTilePipe pipe{nullptr, fe_c_tile64, fe_c_rec64, nullptr, 8, fe_smem, full_bar, &w};
+  FeTilePipe pipe{nullptr, tile_s, fe_c_rec64, nullptr, 8, fe_smem, full_bar, &w};
+  pipe.stage_bytes = STAGE;
   pipe.init_barriers();
   for (;;) {
     if (tid == 0) item_s = int(atomicAdd(counter, 1u));
@@ -91,7 +96,7 @@ __global__ void __launch_bounds__(128, MINB) fe_batch_f64_kernel(const unsigned 
         break;
       }
       int Lt, first, n;
-      fe_item(w, fe_c_tile64, i, Lt, first, n);
+      fe_item(w, tile_s, i, Lt, first, n);
       const double* rec = reinterpret_cast<const double*>(pipe.stage(i));
 #define FE_CB(l) if (l >= LLO && l <= LHI && Lt == l) fe_tile_f64<(l >= LLO && l <= LHI ? l : LLO), NP>(rec, n, cx, cy, cz, acc);
       FE_CB(0) FE_CB(1) FE_CB(2) FE_CB(3) FE_CB(4) FE_CB(5) FE_CB(6) FE_CB(7) FE_CB(8)

@@ -2,10 +2,13 @@
 // and build_table / ESPEngine (fastesp/table.py:176-259, fastesp/esp.py:168-257).
 //
 // One thread per primitive pair.  Work items are grouped by the shell pair's
-// (la, lb) so that a block runs one template instance; each thread writes its
-// pair to a fixed slot of its class's staging array (slots are numbered in
-// the reference's pair order), with a keep flag.  A scan of the flags and a
-// scatter kernel then compact every class in order into the table.
+// (la, lb) so that a block runs one template instance; a pair that survives
+// the screen is written to a fixed slot of its class's staging array (slots
+// are numbered in the reference's pair order), with a keep flag.  A thread
+// spends at most FE_SCREEN_BUDGET box/point tests on the screen; the pairs it
+// leaves undecided are finished by one warp each (fe_screen_pending_kernel).
+// A scan of the flags and a scatter kernel then compact every class in order
+// into the table, deriving the mixed-precision records on the way.
 //
 // Per primitive pair (a = exponent of shell si, b = of sj):
 //   p = a + b, P = (aA + bB)/p, K = exp(-ab/p |A-B|^2)       (esp.py:226-230)
@@ -59,10 +62,18 @@ struct FeBuildArgs {
   const long long* class_slot0;  // first global slot of class L in the staging arrays
   double* stage;                 // staging records, class L at stage_off[L] doubles
   const long long* stage_off;
-  int* keep;                     // per global slot
+  int* keep;                     // per global slot: 0 dropped, 1 kept, 2 pending
   double* srule;                 // per global slot: K (pi/p)^1.5 etab[0]
   int* swork;                    // per global slot: its work item
+  int* pending;                  // slots whose screen ran past the search budget
+  int* npending;                 // their count (capacity: the slot count)
 };
+
+// Box or point tests a thread spends on a pair's screen before it hands the
+// pair to the warp-parallel screen (fe_screen_pending_kernel).  Most pairs are
+// decided within it; the few that need the exact nearest distance over many
+// points would otherwise hold their whole warp (one thread per pair).
+#define FE_SCREEN_BUDGET 64
 
 __constant__ signed char fe_cart[5][15][3] = {
   {{0, 0, 0}},
@@ -141,42 +152,50 @@ FE_DEV double fe_box_lb2(const double* __restrict__ b, const double (&P)[3]) {
 }
 
 // Bounding boxes of consecutive 32-point blocks (level 0: points -> boxes) and
-// of 32-box superblocks (level 1: boxes -> superboxes).  One thread per box.
-__global__ void fe_point_boxes_kernel(const double* __restrict__ pts, int npts, double* box,
-                                      int nbox) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nbox) return;
-  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-  const int q1 = min(32 * b + 32, npts);
-  for (int q = 32 * b; q < q1; ++q)
+// of 32-box superblocks (level 1: boxes -> superboxes).  One warp per box: a
+// lane per member, min/max by shuffles.
+FE_DEV void fe_warp_box(double (&lo)[3], double (&hi)[3]) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      lo[k] = fmin(lo[k], pts[3 * q + k]);
-      hi[k] = fmax(hi[k], pts[3 * q + k]);
+      lo[k] = fmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+      hi[k] = fmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
     }
+}
+
+__global__ void fe_point_boxes_kernel(const double* __restrict__ pts, int npts, double* box,
+                                      int nbox) {
+  const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (b >= nbox) return;                       // whole warps: nbox is per warp
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  const int q = 32 * b + lane;
+  if (q < npts)
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    box[6 * b + k] = lo[k];
-    box[6 * b + 3 + k] = hi[k];
+    for (int k = 0; k < 3; ++k) lo[k] = hi[k] = pts[3 * q + k];
+  fe_warp_box(lo, hi);
+  if (lane < 3) {
+    box[6 * b + lane] = lo[lane];
+    box[6 * b + 3 + lane] = hi[lane];
   }
 }
 
 __global__ void fe_super_boxes_kernel(const double* __restrict__ box, int nbox, double* sbox,
                                       int nsbox) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (s >= nsbox) return;
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-  const int b1 = min(32 * s + 32, nbox);
-  for (int b = 32 * s; b < b1; ++b)
+  const int b = 32 * s + lane;
+  if (b < nbox)
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      lo[k] = fmin(lo[k], box[6 * b + k]);
-      hi[k] = fmax(hi[k], box[6 * b + 3 + k]);
+      lo[k] = box[6 * b + k];
+      hi[k] = box[6 * b + 3 + k];
     }
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    sbox[6 * s + k] = lo[k];
-    sbox[6 * s + 3 + k] = hi[k];
+  fe_warp_box(lo, hi);
+  if (lane < 3) {
+    sbox[6 * s + lane] = lo[lane];
+    sbox[6 * s + 3 + lane] = hi[lane];
   }
 }
 
@@ -208,6 +227,83 @@ FE_DEV void fe_hermite_1d(double ip, double xa, double xb,
         e[i][j][t] = v;
       }
     }
+}
+
+// The reference's point screen (keep unless K bound / max(d, 0.05) < tol,
+// d = dmin or dmin - reff, dmin the exact IEEE minimum of ((dx^2 + dy^2) +
+// dz^2) over the points), decided without the full minimum where the answer
+// is certain: with r* = K bound / tol,
+//  * r* < 0.05 (1 - 1e-9): dropped, whatever dmin is;
+//  * only points within rcut = (r* (1 + 1e-9) [+ reff]) can matter: boxes of
+//    32 points (and superboxes of 1024) whose distance lower bound exceeds
+//    rcut, or the best distance so far, are skipped;
+//  * a point that makes the pair kept with a 1e-9 relative margin ends the
+//    search (kept); no point within rcut means dropped;
+//  * otherwise the minimum over the points within rcut is the exact dmin and
+//    the reference's formula decides.
+// The 1e-9 margins are far above the rounding of the tests themselves.
+struct FeScreen {
+  double KB, tol, rcut2, reff;
+  int rule;
+  bool none;                          // decided "drop" without a search
+  FE_DEV FeScreen(const FeBuildArgs& a, double kb, double rf)
+      : KB(kb), tol(a.tol), rcut2(0.0), reff(rf), rule(a.rule), none(false) {
+    const double rstar = KB / tol;
+    if (rstar < 0.05 * (1.0 - 1e-9)) {
+      none = true;
+    } else {
+      const double rcut = (rstar * (1.0 + 1e-9) + (rule == 1 ? reff : 0.0)) * (1.0 + 1e-12);
+      rcut2 = rcut * rcut;
+    }
+  }
+  FE_DEV static double dist2(const double* q, const double (&P)[3]) {
+    const double dx = __dsub_rn(q[0], P[0]);
+    const double dy = __dsub_rn(q[1], P[1]);
+    const double dz = __dsub_rn(q[2], P[2]);
+    return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+  }
+  FE_DEV bool sure_keep(double d2) const {
+    double d = __dsqrt_rn(d2);
+    if (rule == 1) d = d - reff;
+    return KB >= tol * (1.0 + 1e-9) * fmax(d, 0.05);
+  }
+  // the reference's decision from the exact minimum over the points within rcut
+  FE_DEV bool keep_exact(double d2min) const {
+    if (!(d2min < 1e300)) return false;
+    double dd = __dsqrt_rn(d2min);
+    if (rule == 1) dd = dd - reff;
+    dd = fmax(dd, 0.05);
+    return !(__ddiv_rn(KB, dd) < tol);
+  }
+};
+
+// One thread's screen with a budget of FE_SCREEN_BUDGET box/point tests:
+// 0 dropped, 1 kept, 2 undecided (the warp-parallel screen finishes it).
+FE_DEV int fe_screen_thread(const FeBuildArgs& a, const double (&P)[3], double KB, double reff) {
+  if (a.npts == 0 || a.tol <= 0.0) return 1;        // no points, or tol 0: every pair is kept
+  const FeScreen sc(a, KB, reff);
+  if (sc.none) return 0;
+  double d2min = 1e300;
+  int steps = 0;
+  for (int sb = 0; sb < a.nsbox; ++sb) {
+    if (++steps > FE_SCREEN_BUDGET) return 2;
+    const double ls = fe_box_lb2(a.sbox + 6 * sb, P) * (1.0 - 1e-12);
+    if (ls > sc.rcut2 || ls > d2min) continue;
+    const int b1 = min(32 * sb + 32, a.nbox);
+    for (int b = 32 * sb; b < b1; ++b) {
+      if (++steps > FE_SCREEN_BUDGET) return 2;
+      const double lb = fe_box_lb2(a.box + 6 * b, P) * (1.0 - 1e-12);
+      if (lb > sc.rcut2 || lb > d2min) continue;
+      const int q1 = min(32 * b + 32, a.npts);
+      steps += q1 - 32 * b;
+      for (int q = 32 * b; q < q1; ++q) {
+        const double d2 = FeScreen::dist2(a.pts + 3 * q, P);
+        if (d2 <= sc.rcut2) d2min = fmin(d2min, d2);
+      }
+      if (d2min < 1e300 && sc.sure_keep(d2min)) return 1;
+    }
+  }
+  return sc.keep_exact(d2min) ? 1 : 0;
 }
 
 template <int LA, int LB>
@@ -289,29 +385,22 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
   // sum rule: int rho_pair = K (pi/p)^1.5 etab[0]   (build_pairs.cpp:294-296)
   a.srule[slot] = K * pow(3.14159265358979323846 / p, 1.5) * etab[0];
 
-  // G_k = (2 pi / p) (2p)^m_k sum_t M0[k,t] etab[t]
-  const double cf = 2.0 * 3.14159265358979323846 / p;
   const double tp = 2.0 * p;
-  double pw[L + 1];
-  pw[0] = 1.0;
-#pragma unroll
-  for (int m = 1; m <= L; ++m) pw[m] = pw[m - 1] * tp;
-  double* rec = a.stage + a.stage_off[L] + (slot - a.class_slot0[L]) * REC;
   const short* rp = fe_m0_ptr<L>();
   const short* rc = fe_m0_col<L>();
   const float* rv = fe_m0_val<L>();
   const signed char* rm = fe_m0_m<L>();
-  const short* gpos = fe_gpos<L>();      // record position of term k (consumption order)
-  bool anyg = false;
+  if (a.rule == 1) {
+    // the C++ builder drops pairs whose G are all zero (build_pairs.cpp:309)
+    bool anyg = false;
 #pragma unroll 1
-  for (int k = 0; k < NT; ++k) {
-    double s = 0.0;
-    for (int q = rp[k]; q < rp[k + 1]; ++q) s += double(rv[q]) * etab[rc[q]];
-    const double g = cf * pw[rm[k]] * s;
-    anyg |= (g != 0.0);
-    rec[6 + gpos[k]] = g;
+    for (int k = 0; k < NT && !anyg; ++k) {
+      double sk = 0.0;
+      for (int q = rp[k]; q < rp[k + 1]; ++q) sk += double(rv[q]) * etab[rc[q]];
+      anyg = sk != 0.0;
+    }
+    if (!anyg) return;
   }
-  if (a.rule == 1 && !anyg) return;
 
   // screening bound (esp.py:251-254)
   const double sq = sqrt(tp);
@@ -330,67 +419,24 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
                  * fe_screen_mom[tz]) * sqp[tx + ty + tz];
   const double bound = pow(tp, -1.5) * bsum;
   const double reff = 1.6 * sqrt((L + 2.0) / p);
-
-  // Point screen with the reference's decision (keep unless
-  // K bound / max(d, 0.05) < tol, d = dmin or dmin - reff, dmin the exact
-  // IEEE minimum of ((dx^2 + dy^2) + dz^2) over the points), decided without
-  // the full minimum where the answer is certain: with r* = K bound / tol,
-  //  * r* < 0.05 (1 - 1e-9): dropped, whatever dmin is;
-  //  * only points within rcut = (r* (1 + 1e-9) [+ reff]) can matter: boxes of
-  //    32 points (and superboxes of 1024) whose distance lower bound exceeds
-  //    rcut, or the best distance so far, are skipped;
-  //  * a point that makes the pair kept with a 1e-9 relative margin ends the
-  //    search (kept); no point within rcut means dropped;
-  //  * otherwise the minimum over the points within rcut is the exact dmin and
-  //    the reference's formula decides.
-  // The 1e-9 margins are far above the rounding of the tests themselves.
   const double KB = __dmul_rn(K, bound);
-  double d2min = 1e300;
-  bool sure = false, none = false;
-  auto sure_keep = [&](double d2) {
-    double d = __dsqrt_rn(d2);
-    if (a.rule == 1) d = d - reff;
-    return KB >= a.tol * (1.0 + 1e-9) * fmax(d, 0.05);
-  };
-  if (a.npts > 0 && a.tol > 0.0) {
-    const double rstar = KB / a.tol;
-    if (rstar < 0.05 * (1.0 - 1e-9)) {
-      none = true;
-    } else {
-      const double rcut = (rstar * (1.0 + 1e-9) + (a.rule == 1 ? reff : 0.0)) * (1.0 + 1e-12);
-      const double rcut2 = rcut * rcut;
-      for (int sb = 0; sb < a.nsbox && !sure; ++sb) {
-        const double ls = fe_box_lb2(a.sbox + 6 * sb, P) * (1.0 - 1e-12);
-        if (ls > rcut2 || ls > d2min) continue;
-        const int b1 = min(32 * sb + 32, a.nbox);
-        for (int b = 32 * sb; b < b1; ++b) {
-          const double lb = fe_box_lb2(a.box + 6 * b, P) * (1.0 - 1e-12);
-          if (lb > rcut2 || lb > d2min) continue;
-          const int q1 = min(32 * b + 32, a.npts);
-          for (int q = 32 * b; q < q1; ++q) {
-            const double dx = __dsub_rn(a.pts[3 * q], P[0]);
-            const double dy = __dsub_rn(a.pts[3 * q + 1], P[1]);
-            const double dz = __dsub_rn(a.pts[3 * q + 2], P[2]);
-            const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-            if (d2 <= rcut2) d2min = fmin(d2min, d2);
-          }
-          if (d2min < 1e300 && sure_keep(d2min)) {
-            sure = true;
-            break;
-          }
-        }
-      }
-      none = !sure && !(d2min < 1e300);
-    }
-  } else {
-    sure = true;                       // no points, or tol 0: every pair is kept
+  const int decided = fe_screen_thread(a, P, KB, reff);
+  if (decided == 0) return;
+
+  // G_k = (2 pi / p) (2p)^m_k sum_t M0[k,t] etab[t], at record position fe_gpos_L[k]
+  const double cf = 2.0 * 3.14159265358979323846 / p;
+  double pw[L + 1];
+  pw[0] = 1.0;
+#pragma unroll
+  for (int m = 1; m <= L; ++m) pw[m] = pw[m - 1] * tp;
+  double* rec = a.stage + a.stage_off[L] + (slot - a.class_slot0[L]) * REC;
+  const short* gpos = fe_gpos<L>();
+#pragma unroll 1
+  for (int k = 0; k < NT; ++k) {
+    double sk = 0.0;
+    for (int q = rp[k]; q < rp[k + 1]; ++q) sk += double(rv[q]) * etab[rc[q]];
+    rec[6 + gpos[k]] = cf * pw[rm[k]] * sk;
   }
-  if (none) return;
-  double dd = __dsqrt_rn(d2min);
-  if (a.rule == 1) dd = dd - reff;
-  dd = fmax(dd, 0.05);
-  const bool keep = a.npts == 0 || sure ? true : !(__ddiv_rn(KB, dd) < a.tol);
-  if (!keep) return;
   rec[0] = p;
   rec[1] = P[0];
   rec[2] = P[1];
@@ -399,7 +445,12 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
   rec[5] = KB;
 #pragma unroll
   for (int k = 6 + NT; k < REC; ++k) rec[k] = 0.0;
-  a.keep[slot] = 1;
+  a.keep[slot] = decided;
+  if (decided == 2) {
+    const int at = atomicAdd(a.npending, 1);
+    if (at < int(a.class_slot0[FE_NCLASS])) a.pending[at] = int(slot);
+    else fe_flag(FE_ST_OVERFLOW);
+  }
 }
 
 #define FE_BUILD_THREADS 128
@@ -422,14 +473,180 @@ __global__ void __launch_bounds__(FE_BUILD_THREADS) fe_build_kernel(const FeBuil
   }
 }
 
+// Radius beyond which sum_n b_n / r^(n+1) < tau (b_n >= 0): with u = 1/r the
+// sum is convex and increasing in u, so Newton's method started above the root
+// (at the smallest u where one term alone reaches tau) descends to it
+// monotonically.  0 when every b_n is 0 (never routed); +inf when a b_n is not
+// finite.  Widened by 1e-6 relative so the radius is never below the exact one.
+FE_DEV double fe_route_radius(const double* b, int L, double tau) {
+  double u = 1e300;
+  bool any = false;
+  for (int n = 0; n <= L; ++n) {
+    if (!(b[n] >= 0.0) || isinf(b[n])) return __longlong_as_double(0x7ff0000000000000LL);
+    if (b[n] > 0.0) {
+      u = fmin(u, pow(tau / b[n], 1.0 / double(n + 1)));
+      any = true;
+    }
+  }
+  if (!any) return 0.0;
+  for (int it = 0; it < 100; ++it) {
+    double g = 0.0, dg = 0.0;                 // g = sum b_n u^n and g'(u), Horner
+    for (int n = L; n >= 0; --n) {
+      dg = fma(dg, u, g);
+      g = fma(g, u, b[n]);
+    }
+    const double f = u * g, df = fma(u, dg, g);   // f = u g, f' = g + u g'
+    const double step = (f - tau) / df;
+    if (!(step > 1e-15 * u)) break;
+    u -= step;
+  }
+  return (1.0 + 1e-6) / u;
+}
+
+// FP32 asymptotic Boys thresholds by class, for runtime indexing.
+__constant__ float fe_c_boys32_asym_T[FE_NCLASS] = {
+  fe_boys32_asym_T[0], fe_boys32_asym_T[1], fe_boys32_asym_T[2], fe_boys32_asym_T[3],
+  fe_boys32_asym_T[4], fe_boys32_asym_T[5], fe_boys32_asym_T[6], fe_boys32_asym_T[7],
+  fe_boys32_asym_T[8]};
+
+// The mixed-precision record of one FP64 record ``r`` of class L (layout in
+// table.cuh): coefficients c_k = K G_k s_m p^-(m+1/2) and the routing-bound
+// coefficients formed in FP64, then rounded to float once.  ``tau_fast`` is
+// the routing threshold the far radius is computed for.
+FE_DEV void fe_f32_record(const double* __restrict__ r, float* __restrict__ o, int L,
+                          float tau_fast) {
+  const int R32 = fe_c_rec32[L], NT = fe_c_nterm[L];
+  auto split = [](double v, float& hi, float& lo) {
+    hi = float(v);
+    lo = float(v - double(hi));
+  };
+  const double p = r[0], K = r[4];
+  o[0] = float(p);
+  o[1] = float(sqrt(p));
+#pragma unroll
+  for (int k = 0; k < 3; ++k) split(r[1 + k], o[2 + k], o[5 + k]);
+  o[9] = float(1.0 / sqrt(p));
+  o[10] = o[11] = 0.0f;
+  // s_m = (sqrt(pi)/2) (2m-1)!!/2^m (the FP32 Boys vector is F_m / s_m,
+  // boys.cuh) and p^-(m+1/2): with both folded in, F_m of an asymptotic
+  // point is 1/|R|^(2m+1) exactly
+  double sm[FE_NCLASS], pm[FE_NCLASS];
+  sm[0] = FE_SQRT_PI_2;
+  pm[0] = 1.0 / sqrt(p);
+  for (int m = 1; m <= L; ++m) {
+    sm[m] = sm[m - 1] * (0.5 * double(2 * m - 1));
+    pm[m] = pm[m - 1] / p;
+  }
+  const int c0 = fe_route_off[L];
+  for (int k = 0; k < NT; ++k) {
+    const int m = fe_route_nm[c0 + k] >> 4;
+    o[12 + 2 * k] = o[13 + 2 * k] = float(K * r[6 + k] * sm[m] * pm[m]);
+  }
+  // routing bound: K sum_k |G_k R^a F_m| <= sum_n b_n / |R|^(n+1) with
+  // b_n = K sum_{k: 2m - |a| = n} |G_k| c_k p^-(m + 1/2); rounded up to float
+  double b[FE_NCLASS];
+  for (int q = 0; q <= L; ++q) b[q] = 0.0;
+  for (int k = 0; k < NT; ++k) {
+    const unsigned nm = fe_route_nm[c0 + k];
+    b[nm & 15u] += fabs(r[6 + k]) * fe_route_c[c0 + k] * pm[nm >> 4];
+  }
+  for (int q = 0; q <= L; ++q) {
+    o[12 + 2 * NT + q] = __double2float_ru(K * b[q]);
+    b[q] = double(o[12 + 2 * NT + q]);
+  }
+  // far radius: the FP32 Boys vector is asymptotic (T = p r^2 beyond the
+  // class's FP32 threshold) and the bound (with the stored, rounded-up b_n)
+  // is below tau_fast
+  const double rt = fe_route_radius(b, L, double(tau_fast));
+  const double ra2 = double(fe_c_boys32_asym_T[L]) / p * (1.0 + 1e-6);
+  o[8] = __double2float_ru(fmax(ra2, rt * rt));
+  for (int k = 13 + 2 * NT + L; k < R32; ++k) o[k] = 0.0f;
+}
+
+// Mixed-precision records of a table whose FP64 records are in place (an
+// imported table): fe_f32_record per record.
+__global__ void fe_make_f32_kernel(unsigned char* table, float tau_fast) {
+  FeTableHdr* hdr = reinterpret_cast<FeTableHdr*>(table);
+  const int L = blockIdx.y;
+  const int n = hdr->count[L];
+  const double* src = reinterpret_cast<const double*>(table + hdr->off64[L]);
+  float* dst = reinterpret_cast<float*>(table + hdr->off32[L]);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    fe_f32_record(src + size_t(i) * fe_c_rec64[L], dst + size_t(i) * fe_c_rec32[L], L, tau_fast);
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+    hdr->has32 = 1;
+    hdr->tau_fast = tau_fast;
+  }
+}
+
+// One warp per pair that its thread left undecided (fe_screen_thread ran past
+// its budget): the same decision, searched by 32 lanes -- superboxes across
+// the lanes, then the boxes of each candidate superbox, then the points of
+// each candidate box -- in the serial search's order.  d2min, the minimum over
+// the points within rcut found so far, is the same in every lane (a shuffle
+// reduction), so the pruning and the final decision are the serial search's.
+__global__ void __launch_bounds__(128) fe_screen_pending_kernel(const FeBuildArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int warp = int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nwarp = int((gridDim.x * blockDim.x) >> 5);
+  const int np = min(*a.npending, int(a.class_slot0[FE_NCLASS]));
+  for (int i = warp; i < np; i += nwarp) {
+    const long long slot = a.pending[i];
+    int L = 0;
+    while (L + 1 < FE_NCLASS && slot >= a.class_slot0[L + 1]) ++L;
+    const double* rec = a.stage + a.stage_off[L] + (slot - a.class_slot0[L]) * fe_c_rec64[L];
+    const double P[3] = {rec[1], rec[2], rec[3]};
+    const FeScreen sc(a, rec[5], 1.6 * sqrt((L + 2.0) / rec[0]));
+    double d2min = 1e300;
+    bool sure = sc.none;                      // (cannot happen: its thread searched)
+    for (int sb0 = 0; sb0 < a.nsbox && !sure; sb0 += 32) {
+      bool cand = false;
+      if (sb0 + lane < a.nsbox) {
+        const double ls = fe_box_lb2(a.sbox + 6 * (sb0 + lane), P) * (1.0 - 1e-12);
+        cand = ls <= sc.rcut2 && ls <= d2min;
+      }
+      unsigned cm = __ballot_sync(0xffffffffu, cand);
+      while (cm && !sure) {
+        const int sbi = sb0 + __ffs(cm) - 1;
+        cm &= cm - 1;
+        if (fe_box_lb2(a.sbox + 6 * sbi, P) * (1.0 - 1e-12) > d2min) continue;
+        const int b = 32 * sbi + lane;
+        bool bc = false;
+        if (b < a.nbox) {
+          const double lb = fe_box_lb2(a.box + 6 * b, P) * (1.0 - 1e-12);
+          bc = lb <= sc.rcut2 && lb <= d2min;
+        }
+        unsigned bm = __ballot_sync(0xffffffffu, bc);
+        while (bm && !sure) {
+          const int bi = 32 * sbi + __ffs(bm) - 1;
+          bm &= bm - 1;
+          if (fe_box_lb2(a.box + 6 * bi, P) * (1.0 - 1e-12) > d2min) continue;
+          const int q = 32 * bi + lane;
+          double d2 = 1e300;
+          if (q < a.npts) {
+            d2 = FeScreen::dist2(a.pts + 3 * q, P);
+            if (!(d2 <= sc.rcut2)) d2 = 1e300;
+          }
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) d2 = fmin(d2, __shfl_xor_sync(0xffffffffu, d2, o));
+          d2min = fmin(d2min, d2);
+          sure = d2min < 1e300 && sc.sure_keep(d2min);
+        }
+      }
+    }
+    if (lane == 0) a.keep[slot] = (sure || sc.keep_exact(d2min)) ? 1 : 0;
+  }
+}
+
 // Move kept staging records of every class, in slot order, into the table,
-// and record each one's work item in the table's source section.
+// derive their mixed-precision records, and record each one's work item in
+// the table's source section.
 // ``pos`` is the exclusive scan of ``keep`` over all global slots.
 __global__ void fe_scatter_kernel(const double* __restrict__ stage, const long long* stage_off,
                                   const long long* class_slot0, int nclass,
                                   const int* __restrict__ keep, const int* __restrict__ pos,
                                   const int* __restrict__ swork, long long nslot,
-                                  unsigned char* table) {
+                                  unsigned char* table, float tau_fast) {
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s >= nslot || !keep[s]) return;
   int L = 0;
@@ -441,6 +658,8 @@ __global__ void fe_scatter_kernel(const double* __restrict__ stage, const long l
   const double* src = stage + stage_off[L] + (s - class_slot0[L]) * R;
   double* out = reinterpret_cast<double*>(table + hdr->off64[L]) + size_t(dst) * R;
   for (int k = 0; k < R; ++k) out[k] = src[k];
+  fe_f32_record(src, reinterpret_cast<float*>(table + hdr->off32[L]) + size_t(dst) * fe_c_rec32[L],
+                L, tau_fast);
   long long base = 0;
   for (int l = 0; l < L; ++l) base += hdr->cap[l];
   reinterpret_cast<int*>(table + hdr->off_src)[base + dst] = swork[s];
@@ -451,7 +670,8 @@ __global__ void fe_scatter_kernel(const double* __restrict__ stage, const long l
 // the partial sums, so the result does not depend on scheduling.
 __global__ void __launch_bounds__(1024) fe_finalize_kernel(
     const long long* class_slot0, int nclass, long long nslot, const int* __restrict__ keep,
-    const int* __restrict__ pos, const double* __restrict__ srule, unsigned char* table) {
+    const int* __restrict__ pos, const double* __restrict__ srule, unsigned char* table,
+    float tau_fast) {
   __shared__ double red[1024];
   FeTableHdr* hdr = reinterpret_cast<FeTableHdr*>(table);
   const int t = threadIdx.x;
@@ -470,6 +690,8 @@ __global__ void __launch_bounds__(1024) fe_finalize_kernel(
   if (t == 0) {
     hdr->sum_rule = red[0];
     hdr->has_src = 1;
+    hdr->has32 = 1;                      // the scatter wrote the FP32 records
+    hdr->tau_fast = tau_fast;
   }
 }
 
@@ -530,104 +752,3 @@ __global__ void __launch_bounds__(FE_SCAN_BLOCK) fe_scan_apply_kernel(
   if (i < n) pos[i] = bsum[blockIdx.x] + buf[threadIdx.x] - v;
 }
 
-// Radius beyond which sum_n b_n / r^(n+1) < tau (b_n >= 0): with u = 1/r the
-// sum is convex and increasing in u, so Newton's method started above the root
-// (at the smallest u where one term alone reaches tau) descends to it
-// monotonically.  0 when every b_n is 0 (never routed); +inf when a b_n is not
-// finite.  Widened by 1e-6 relative so the radius is never below the exact one.
-FE_DEV double fe_route_radius(const double* b, int L, double tau) {
-  double u = 1e300;
-  bool any = false;
-  for (int n = 0; n <= L; ++n) {
-    if (!(b[n] >= 0.0) || isinf(b[n])) return __longlong_as_double(0x7ff0000000000000LL);
-    if (b[n] > 0.0) {
-      u = fmin(u, pow(tau / b[n], 1.0 / double(n + 1)));
-      any = true;
-    }
-  }
-  if (!any) return 0.0;
-  for (int it = 0; it < 100; ++it) {
-    double g = 0.0, dg = 0.0;                 // g = sum b_n u^n and g'(u), Horner
-    for (int n = L; n >= 0; --n) {
-      dg = fma(dg, u, g);
-      g = fma(g, u, b[n]);
-    }
-    const double f = u * g, df = fma(u, dg, g);   // f = u g, f' = g + u g'
-    const double step = (f - tau) / df;
-    if (!(step > 1e-15 * u)) break;
-    u -= step;
-  }
-  return (1.0 + 1e-6) / u;
-}
-
-// FP32 asymptotic Boys thresholds by class, for runtime indexing.
-__constant__ float fe_c_boys32_asym_T[FE_NCLASS] = {
-  fe_boys32_asym_T[0], fe_boys32_asym_T[1], fe_boys32_asym_T[2], fe_boys32_asym_T[3],
-  fe_boys32_asym_T[4], fe_boys32_asym_T[5], fe_boys32_asym_T[6], fe_boys32_asym_T[7],
-  fe_boys32_asym_T[8]};
-
-// Mixed-precision records from the FP64 records (layout in table.cuh):
-// coefficients c_k = K G_k s_m p^-(m+1/2) and the routing-bound coefficients
-// formed in FP64, then rounded to float once.  ``tau_fast`` is the routing
-// threshold the far radius is computed for.
-__global__ void fe_make_f32_kernel(unsigned char* table, float tau_fast) {
-  FeTableHdr* hdr = reinterpret_cast<FeTableHdr*>(table);
-  const int L = blockIdx.y;
-  const int n = hdr->count[L];
-  const int R64 = fe_c_rec64[L], R32 = fe_c_rec32[L], NT = fe_c_nterm[L];
-  const double* src = reinterpret_cast<const double*>(table + hdr->off64[L]);
-  float* dst = reinterpret_cast<float*>(table + hdr->off32[L]);
-  auto split = [](double v, float& hi, float& lo) {
-    hi = float(v);
-    lo = float(v - double(hi));
-  };
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double* r = src + size_t(i) * R64;
-    float* o = dst + size_t(i) * R32;
-    const double p = r[0], K = r[4];
-    o[0] = float(p);
-    o[1] = float(sqrt(p));
-#pragma unroll
-    for (int k = 0; k < 3; ++k) split(r[1 + k], o[2 + k], o[5 + k]);
-    o[9] = float(1.0 / sqrt(p));
-    o[10] = o[11] = 0.0f;
-    // s_m = (sqrt(pi)/2) (2m-1)!!/2^m (the FP32 Boys vector is F_m / s_m,
-    // boys.cuh) and p^-(m+1/2): with both folded in, F_m of an asymptotic
-    // point is 1/|R|^(2m+1) exactly
-    double sm[FE_NCLASS], pm[FE_NCLASS];
-    sm[0] = FE_SQRT_PI_2;
-    pm[0] = 1.0 / sqrt(p);
-    for (int m = 1; m <= L; ++m) {
-      sm[m] = sm[m - 1] * (0.5 * double(2 * m - 1));
-      pm[m] = pm[m - 1] / p;
-    }
-    const int c0 = fe_route_off[L];
-    for (int k = 0; k < NT; ++k) {
-      const int m = fe_route_nm[c0 + k] >> 4;
-      o[12 + 2 * k] = o[13 + 2 * k] = float(K * r[6 + k] * sm[m] * pm[m]);
-    }
-    // routing bound: K sum_k |G_k R^a F_m| <= sum_n b_n / |R|^(n+1) with
-    // b_n = K sum_{k: 2m - |a| = n} |G_k| c_k p^-(m + 1/2); rounded up to float
-    double b[FE_NCLASS];
-    for (int q = 0; q <= L; ++q) b[q] = 0.0;
-    for (int k = 0; k < NT; ++k) {
-      const unsigned nm = fe_route_nm[c0 + k];
-      b[nm & 15u] += fabs(r[6 + k]) * fe_route_c[c0 + k] * pm[nm >> 4];
-    }
-    for (int q = 0; q <= L; ++q) {
-      o[12 + 2 * NT + q] = __double2float_ru(K * b[q]);
-      b[q] = double(o[12 + 2 * NT + q]);
-    }
-    // far radius: the FP32 Boys vector is asymptotic (T = p r^2 beyond the
-    // class's FP32 threshold) and the bound (with the stored, rounded-up b_n)
-    // is below tau_fast
-    const double rt = fe_route_radius(b, L, double(tau_fast));
-    const double ra2 = double(fe_c_boys32_asym_T[L]) / p * (1.0 + 1e-6);
-    o[8] = __double2float_ru(fmax(ra2, rt * rt));
-    for (int k = 13 + 2 * NT + L; k < R32; ++k) o[k] = 0.0f;
-  }
-  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
-    hdr->has32 = 1;
-    hdr->tau_fast = tau_fast;
-  }
-}

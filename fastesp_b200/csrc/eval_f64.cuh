@@ -146,6 +146,7 @@ struct FeTilePipe {
   const int64_t* off2 = nullptr;
   int elem2 = 0;
   int base = 0;
+  int stage_bytes = FE_STAGE_BYTES;   // bytes per ring stage (the tile sizes follow it)
 
   FE_DEV void init_barriers() const {
     if (threadIdx.x == 0) {
@@ -171,10 +172,10 @@ struct FeTilePipe {
     const unsigned bytes = unsigned(n) * unsigned(rec[L]) * unsigned(elem);
     const unsigned bytes2 = rec2 ? unsigned(n) * unsigned(rec2[L]) * unsigned(elem2) : 0u;
     mbar_expect_tx(&bar[s], bytes + bytes2);
-    bulk_g2s(smem + s * FE_STAGE_BYTES, table + off[L] + size_t(first) * rec[L] * elem, bytes,
+    bulk_g2s(smem + s * stage_bytes, table + off[L] + size_t(first) * rec[L] * elem, bytes,
              &bar[s]);
     if (rec2)
-      bulk_g2s(smem + s * FE_STAGE_BYTES + bytes, table + off2[L] + size_t(first) * rec2[L] * elem2,
+      bulk_g2s(smem + s * stage_bytes + bytes, table + off2[L] + size_t(first) * rec2[L] * elem2,
                bytes2, &bar[s]);
   }
   // Wait for tile i; false (for every thread) if the wait gave up.
@@ -184,7 +185,7 @@ struct FeTilePipe {
     return !__syncthreads_or(!got);
   }
   FE_DEV const unsigned char* stage(int i) const {
-    return smem + ((base + i) % FE_NSTAGE) * FE_STAGE_BYTES;
+    return smem + ((base + i) % FE_NSTAGE) * stage_bytes;
   }
   FE_DEV void release(int i) const {
     __syncthreads();

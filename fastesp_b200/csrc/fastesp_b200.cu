@@ -226,6 +226,7 @@ struct fe_plan {
   size_t table_bytes = 0;
   size_t o_tab64[FE_NCLASS], o_tab32[FE_NCLASS], o_atoms = 0;
   size_t ws_stage = 0, ws_keep = 0, ws_pos = 0, ws_srule = 0, ws_swork = 0, ws_bsum = 0;
+  size_t ws_pending = 0, ws_npend = 0;
   long long nscan_blocks = 0;
   size_t ws_bytes = 0;
 };
@@ -383,6 +384,8 @@ int fe_plan_create(const fe_basis* b, fe_plan** out) {
   p->ws_pos = wput(size_t(p->nslot + 1) * sizeof(int));
   p->ws_srule = wput(size_t(p->nslot + 1) * sizeof(double));
   p->ws_swork = wput(size_t(p->nslot + 1) * sizeof(int));
+  p->ws_pending = wput(size_t(p->nslot + 1) * sizeof(int));
+  p->ws_npend = wput(sizeof(int));
   p->nscan_blocks = (p->nslot + FE_SCAN_BLOCK - 1) / FE_SCAN_BLOCK;
   p->ws_bsum = wput(size_t(p->nscan_blocks + 1) * sizeof(int));
   p->ws_bytes = std::max<size_t>(w, 256);
@@ -476,19 +479,25 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
   a.keep = reinterpret_cast<int*>(wb + p->ws_keep);
   a.srule = reinterpret_cast<double*>(wb + p->ws_srule);
   a.swork = reinterpret_cast<int*>(wb + p->ws_swork);
+  a.pending = reinterpret_cast<int*>(wb + p->ws_pending);
+  a.npending = reinterpret_cast<int*>(wb + p->ws_npend);
   a.nbox = (n_pts + 31) / 32;
   a.nsbox = (a.nbox + 31) / 32;
   double* box = reinterpret_cast<double*>(wb + p->ws_bytes);
   double* sbox = reinterpret_cast<double*>(wb + p->ws_bytes + align256(size_t(a.nbox) * 6 * sizeof(double)));
   a.box = box;
   a.sbox = sbox;
-  if (a.nbox > 0) {
-    fe_point_boxes_kernel<<<(a.nbox + 127) / 128, 128, 0, st>>>(d_pts, n_pts, box, a.nbox);
-    fe_super_boxes_kernel<<<(a.nsbox + 127) / 128, 128, 0, st>>>(box, a.nbox, sbox, a.nsbox);
+  if (a.nbox > 0) {            // one warp per box and per superbox
+    fe_point_boxes_kernel<<<(a.nbox + 3) / 4, 128, 0, st>>>(d_pts, n_pts, box, a.nbox);
+    fe_super_boxes_kernel<<<(a.nsbox + 3) / 4, 128, 0, st>>>(box, a.nbox, sbox, a.nsbox);
     FE_CUDA(cudaGetLastError());
   }
+  FE_CUDA(cudaMemsetAsync(a.npending, 0, sizeof(int), st));
   if (p->nblocks > 0) {
     fe_build_kernel<<<p->nblocks, FE_BUILD_THREADS, 0, st>>>(a);
+    FE_CUDA(cudaGetLastError());
+    // pairs whose screen ran past the per-thread budget: one warp each
+    fe_screen_pending_kernel<<<sm_count() * 8, 128, 0, st>>>(a);
     FE_CUDA(cudaGetLastError());
   }
   int* pos = reinterpret_cast<int*>(wb + p->ws_pos);
@@ -501,13 +510,12 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
     FE_CUDA(cudaGetLastError());
     const int thr = 256;
     fe_scatter_kernel<<<unsigned((p->nslot + thr - 1) / thr), thr, 0, st>>>(
-        a.stage, a.stage_off, a.class_slot0, FE_NCLASS, a.keep, pos, a.swork, p->nslot, tb);
+        a.stage, a.stage_off, a.class_slot0, FE_NCLASS, a.keep, pos, a.swork, p->nslot, tb,
+        float(kTauDefault));
     FE_CUDA(cudaGetLastError());
   }
-  fe_finalize_kernel<<<1, 1024, 0, st>>>(a.class_slot0, FE_NCLASS, p->nslot, a.keep, pos, a.srule, tb);
-  FE_CUDA(cudaGetLastError());
-  fe_make_f32_kernel<<<dim3(std::max(1, 2 * sm_count() / FE_NCLASS), FE_NCLASS), 256, 0, st>>>(
-      tb, float(kTauDefault));
+  fe_finalize_kernel<<<1, 1024, 0, st>>>(a.class_slot0, FE_NCLASS, p->nslot, a.keep, pos, a.srule,
+                                         tb, float(kTauDefault));
   FE_CUDA(cudaGetLastError());
   return FE_OK;
 }
@@ -1140,6 +1148,7 @@ int fe_esp_adjoint(const fe_plan* p, const void* d_plan, const void* d_table,
 // ---------------------------------------------------------------------------
 struct fe_batch {
   int np = 2;
+  int stage = FE_STAGE_BYTES;            // pair-tile (ring stage) bytes
   int grid[2] = {1, 1};
   std::vector<FeBatchMolDev> mols;
   std::vector<FeBatchItem> items[2];     // classes 0..FE_LSPLIT, the g-shell classes
@@ -1154,21 +1163,29 @@ namespace {
 
 constexpr size_t kBatchCounterBytes = 256;   // two counters, one per kernel instance
 
-template <int NP>
+template <int NP, int STAGE>
 struct BatchKernels {
   static constexpr int kMinB = NP == 1 ? 4 : kMinB64;
   static const void* main() {
-    return reinterpret_cast<const void*>(fe_batch_f64_kernel<NP, kMinB, 0, FE_LSPLIT, 0>);
+    return reinterpret_cast<const void*>(fe_batch_f64_kernel<NP, kMinB, 0, FE_LSPLIT, 0, STAGE>);
   }
   static const void* high() {
-    return reinterpret_cast<const void*>(fe_batch_f64_kernel<NP, 1, FE_LSPLIT + 1, FE_NCLASS - 1, 1>);
+    return reinterpret_cast<const void*>(
+        fe_batch_f64_kernel<NP, 1, FE_LSPLIT + 1, FE_NCLASS - 1, 1, STAGE>);
   }
 };
 
-int batch_kernels(int np, const void*& k0, const void*& k1) {
-  if (np == 1) { k0 = BatchKernels<1>::main(); k1 = BatchKernels<1>::high(); return FE_OK; }
-  if (np == 2) { k0 = BatchKernels<2>::main(); k1 = BatchKernels<2>::high(); return FE_OK; }
-  return fail(FE_ERR_ARG, "fe_batch_create: points_per_thread must be 1 or 2");
+int batch_kernels(int np, int stage, const void*& k0, const void*& k1) {
+#define FE_BK(n, sb)                                  \
+  if (np == n && stage == sb) {                        \
+    k0 = BatchKernels<n, sb>::main();                  \
+    k1 = BatchKernels<n, sb>::high();                  \
+    return FE_OK;                                      \
+  }
+  FE_BK(1, 8192) FE_BK(1, 16384) FE_BK(1, 32768) FE_BK(2, 8192) FE_BK(2, 16384) FE_BK(2, 32768)
+#undef FE_BK
+  if (np != 1 && np != 2) return fail(FE_ERR_ARG, "fe_batch_create: points_per_thread must be 1 or 2");
+  return fail(FE_ERR_ARG, "fe_batch_create: stage_bytes must be 8192, 16384 or 32768");
 }
 
 // Algorithmic FLOPs of one (pair, point) evaluation of class L.
@@ -1187,14 +1204,15 @@ int fe_batch_create(const fe_batch_mol* in, int n_mol, const fe_batch_shape* sha
   *out = nullptr;
   const int np = shape ? shape->points_per_thread : 2;
   const int waves = shape ? shape->waves : 4;
+  const int stage = shape && shape->stage_bytes ? shape->stage_bytes : FE_STAGE_BYTES;
   if (waves < 1 || waves > 64) return fail(FE_ERR_ARG, "fe_batch_create: waves must be in 1..64");
   const void* k0 = nullptr;
   const void* k1 = nullptr;
   {
-    const int rc = batch_kernels(np, k0, k1);
+    const int rc = batch_kernels(np, stage, k0, k1);
     if (rc != FE_OK) return rc;
   }
-  const int smem = FE_NSTAGE * FE_STAGE_BYTES;
+  const int smem = FE_NSTAGE * stage;
   FE_CUDA(cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   FE_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int occ0 = 0, occ1 = 0;
@@ -1205,6 +1223,7 @@ int fe_batch_create(const fe_batch_mol* in, int n_mol, const fe_batch_shape* sha
 
   auto* b = new fe_batch();
   b->np = np;
+  b->stage = stage;
   const int ppb = 128 * np;
   std::vector<std::array<int, FE_NCLASS>> cnt(n_mol);
   double total = 0.0;
@@ -1330,7 +1349,7 @@ int fe_batch_run(const fe_batch* b, const void* d_desc, void* d_ws, size_t ws_by
   const void* k0 = nullptr;
   const void* k1 = nullptr;
   {
-    const int rc = batch_kernels(b->np, k0, k1);
+    const int rc = batch_kernels(b->np, b->stage, k0, k1);
     if (rc != FE_OK) return rc;
   }
   unsigned char* wb = static_cast<unsigned char*>(d_ws);
@@ -1338,7 +1357,7 @@ int fe_batch_run(const fe_batch* b, const void* d_desc, void* d_ws, size_t ws_by
   double* partial = reinterpret_cast<double*>(wb + kBatchCounterBytes);
   const unsigned char* desc = static_cast<const unsigned char*>(d_desc);
   FE_CUDA(cudaMemsetAsync(counter, 0, kBatchCounterBytes, st));
-  const int smem = FE_NSTAGE * FE_STAGE_BYTES;
+  const int smem = FE_NSTAGE * b->stage;
   unsigned* c1 = counter + 32;
   if (!b->items[0].empty()) {
     void* a0[] = {&desc, &counter, &partial};

@@ -255,6 +255,9 @@ typedef struct fe_batch_mol {
 typedef struct fe_batch_shape {
   int points_per_thread;        /* 1 or 2: point block of 128 or 256 points */
   int waves;                    /* work items per resident block, 1..64 */
+  int stage_bytes;              /* pair tile: bytes per shared-memory stage, 8192, 16384
+                                   or 32768 (0: 16384); a tile holds stage_bytes / record
+                                   bytes pairs of a class */
 } fe_batch_shape;
 
 typedef struct fe_batch fe_batch;   /* opaque, host memory */

@@ -76,3 +76,10 @@ def test_batch_with_empty_and_tiny_members(batch12, small_system):
     assert vals[3].numel() == 0
     np.testing.assert_allclose(vals[4].cpu().numpy(), g["esp_t12"][:5], rtol=0, atol=1e-12)
     _check(vals[:3], tabs[:3], pts[:3])
+
+
+def test_batch_rejects_unknown_pair_tile(batch12):
+    tabs, pts = batch12
+    with pytest.raises(_lib.FeError) as e:
+        BatchESP(tabs[:2], pts[:2], shape=(2, 4, 12288), graph=False)
+    assert "stage_bytes" in str(e.value)
