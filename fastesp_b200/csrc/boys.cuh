@@ -20,7 +20,8 @@
 //                            3e-17 relative), then the stable downward recursion
 //                            F_(m-1) = (2T F_m + e^-T)/(2m-1).
 //
-// exp and rsqrt are CUDA's own; the grid values F_n(i/16) are 40-digit
+// rsqrt is CUDA's own; e^-T comes from a table of e^(-i/16) and a short Taylor
+// polynomial (fe_exp_neg); the grid values F_n(i/16) and e^(-i/16) are 40-digit
 // reference values generated into classes_gen.cuh.
 #pragma once
 #include "common.cuh"
@@ -41,6 +42,24 @@ FE_DEV double fe_erfc_asym_series(double u) {
   return s;
 }
 
+// e^-T for 0 <= T < 64 from a table of e^(-i h) on the Boys grid (h = 1/16,
+// 40-digit values) times the 8-term Taylor polynomial of e^d, d = i h - T,
+// |d| <= 1/32 (truncation below 3e-17 relative): the table-driven method of
+// P. T. P. Tang (ACM TOMS 15, 1989) with a finer table and no reduction step.
+// ``i`` is round(T / h), in range.
+FE_DEV double fe_exp_neg(double T, int i) {
+  const double d = double(i) * FE_BOYS_GRID_H - T;      // exact
+  double e = 1.0 / 5040.0;
+  e = fma(e, d, 1.0 / 720.0);
+  e = fma(e, d, 1.0 / 120.0);
+  e = fma(e, d, 1.0 / 24.0);
+  e = fma(e, d, 1.0 / 6.0);
+  e = fma(e, d, 0.5);
+  e = fma(e, d, 1.0);
+  e = fma(e, d, 1.0);
+  return __ldg(fe_exp_grid + i) * e;
+}
+
 template <int M>
 FE_DEV void fe_boys_f64(const double T, double (&F)[M + 1]) {
   constexpr double t_asym = fe_boys_asym_T[M];
@@ -53,7 +72,8 @@ FE_DEV void fe_boys_f64(const double T, double (&F)[M + 1]) {
   } else if (T >= FE_BOYS_GRID_TMAX) {
     const double r = rsqrt(T);
     const double h = 0.5 * r * r;
-    const double e = exp(-T);
+    // T < t_asym <= 64 here
+    const double e = fe_exp_neg(T, min(__double2int_rn(T * FE_BOYS_GRID_INV_H), FE_EXP_NROW - 1));
     F[0] = fma(-h * e, fe_erfc_asym_series(h + h), FE_SQRT_PI_2 * r);
 #pragma unroll
     for (int m = 0; m < M; ++m) F[m + 1] = fma(double(2 * m + 1), F[m], -e) * h;
@@ -68,7 +88,7 @@ FE_DEV void fe_boys_f64(const double T, double (&F)[M + 1]) {
     for (int k = FE_BOYS_TAYLOR_K - 2; k >= 0; --k)
       f = fma(f, d * (1.0 / double(k + 1)), __ldg(row + k));
     F[M] = f;
-    const double e = exp(-T);
+    const double e = fe_exp_neg(T, i);
     const double t2 = T + T;
 #pragma unroll
     for (int m = M; m > 0; --m) F[m - 1] = fma(t2, F[m], e) * (1.0 / double(2 * m - 1));

@@ -75,6 +75,8 @@ struct FeBuildArgs {
 // points would otherwise hold their whole warp (one thread per pair).
 #define FE_SCREEN_BUDGET 64
 
+#define FE_SCAN_BLOCK 1024     // slots per block of the keep-flag scan
+
 __constant__ signed char fe_cart[5][15][3] = {
   {{0, 0, 0}},
   {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}},
@@ -151,6 +153,18 @@ FE_DEV double fe_box_lb2(const double* __restrict__ b, const double (&P)[3]) {
   return s;
 }
 
+// Squared distance from P to the farthest corner of the box [lo, hi]: an upper
+// bound of the squared distance to every point in it.
+FE_DEV double fe_box_ub2(const double* __restrict__ b, const double (&P)[3]) {
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double g = fmax(fabs(P[k] - b[k]), fabs(b[3 + k] - P[k]));
+    s += g * g;
+  }
+  return s;
+}
+
 // Bounding boxes of consecutive 32-point blocks (level 0: points -> boxes) and
 // of 32-box superblocks (level 1: boxes -> superboxes).  One warp per box: a
 // lane per member, min/max by shuffles.
@@ -197,6 +211,96 @@ __global__ void fe_super_boxes_kernel(const double* __restrict__ box, int nbox, 
     sbox[6 * s + lane] = lo[lane];
     sbox[6 * s + 3 + lane] = hi[lane];
   }
+}
+
+// The screen's points in a spatially coherent order.  The screen's decision
+// depends on the point set only, not its order, but its 32-point boxes are
+// only as tight as consecutive points are close: callers' point orders (a
+// Fibonacci spiral per atom, a grid row) give boxes spanning a whole sphere.
+// The points are bucketed by the Morton code of a 16 x 16 x 16 grid of cells
+// over their bounding box (a counting sort; the order within a cell does not
+// matter to the screen).
+#define FE_SORT_CELLS 4096
+
+// Partial bounding boxes of the points: block b writes [lo, hi] of its
+// grid-stride share to bb[6 b..6 b + 5]; fe_points_count_kernel combines the
+// FE_BBOX_BLOCKS partials.
+#define FE_BBOX_BLOCKS 64
+__global__ void __launch_bounds__(256) fe_points_bbox_kernel(const double* __restrict__ pts,
+                                                             int npts, double* __restrict__ bb) {
+  __shared__ double red[6][8];
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < npts; q += gridDim.x * blockDim.x)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = fmin(lo[k], pts[3 * q + k]);
+      hi[k] = fmax(hi[k], pts[3 * q + k]);
+    }
+  fe_warp_box(lo, hi);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      red[k][w] = lo[k];
+      red[3 + k][w] = hi[k];
+    }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double l = 1e300, h = -1e300;
+    for (int i = 0; i < 8; ++i) {
+      l = fmin(l, red[threadIdx.x][i]);
+      h = fmax(h, red[3 + threadIdx.x][i]);
+    }
+    bb[6 * blockIdx.x + threadIdx.x] = l;
+    bb[6 * blockIdx.x + 3 + threadIdx.x] = h;
+  }
+}
+
+FE_DEV int fe_morton_cell(const double* __restrict__ q, const double* __restrict__ bb) {
+  int code = 0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double ext = bb[3 + k] - bb[k];
+    const double cs = ext > 0.0 ? ext * (1.0 / 16.0) * (1.0 + 1e-9) : 1.0;
+    // fmax/fmin first: a NaN coordinate goes to cell 0
+    const int c = int(fmin(fmax((q[k] - bb[k]) / cs, 0.0), 15.0));
+#pragma unroll
+    for (int b = 0; b < 4; ++b) code |= ((c >> b) & 1) << (3 * b + k);
+  }
+  return code;
+}
+
+__global__ void fe_points_count_kernel(const double* __restrict__ pts, int npts,
+                                       const double* __restrict__ bbp, int* __restrict__ cell,
+                                       int* __restrict__ count) {
+  __shared__ double bb[6];
+  if (threadIdx.x < 6) {
+    double v = threadIdx.x < 3 ? 1e300 : -1e300;
+    for (int i = 0; i < FE_BBOX_BLOCKS; ++i)
+      v = threadIdx.x < 3 ? fmin(v, bbp[6 * i + threadIdx.x]) : fmax(v, bbp[6 * i + threadIdx.x]);
+    bb[threadIdx.x] = v;
+  }
+  __syncthreads();
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= npts) return;
+  const int c = fe_morton_cell(pts + 3 * q, bb);
+  cell[q] = c;
+  atomicAdd(count + c, 1);
+}
+
+// ``cursor`` starts as the exclusive scan of the cell counts.
+__global__ void fe_points_place_kernel(const double* __restrict__ pts, int npts,
+                                       const int* __restrict__ cell, int* __restrict__ cursor,
+                                       double* __restrict__ out) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= npts) return;
+  const int at = atomicAdd(cursor + cell[q], 1);
+  if (at < 0 || at >= npts) {
+    fe_flag(FE_ST_OVERFLOW);
+    return;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) out[3 * at + k] = pts[3 * q + k];
 }
 
 // E[i][j][t] of (u + xa)^i (u + xb)^j exp(-p u^2), i <= LA, j <= LB, t <= LA+LB.
@@ -267,6 +371,15 @@ struct FeScreen {
     if (rule == 1) d = d - reff;
     return KB >= tol * (1.0 + 1e-9) * fmax(d, 0.05);
   }
+  // Every point of a (non-empty) box whose farthest corner is at squared
+  // distance ub2 passes sure_keep: the corner distance, widened by 1e-12 for
+  // rounding, meets the test with twice its margin.  Then the pair is kept
+  // without looking at the points.
+  FE_DEV bool sure_box(double ub2) const {
+    double d = sqrt(ub2) * (1.0 + 1e-12);
+    if (rule == 1) d = d - reff;
+    return KB >= tol * (1.0 + 2e-9) * fmax(d, 0.05);
+  }
   // the reference's decision from the exact minimum over the points within rcut
   FE_DEV bool keep_exact(double d2min) const {
     if (!(d2min < 1e300)) return false;
@@ -289,11 +402,13 @@ FE_DEV int fe_screen_thread(const FeBuildArgs& a, const double (&P)[3], double K
     if (++steps > FE_SCREEN_BUDGET) return 2;
     const double ls = fe_box_lb2(a.sbox + 6 * sb, P) * (1.0 - 1e-12);
     if (ls > sc.rcut2 || ls > d2min) continue;
+    if (sc.sure_box(fe_box_ub2(a.sbox + 6 * sb, P))) return 1;
     const int b1 = min(32 * sb + 32, a.nbox);
     for (int b = 32 * sb; b < b1; ++b) {
       if (++steps > FE_SCREEN_BUDGET) return 2;
       const double lb = fe_box_lb2(a.box + 6 * b, P) * (1.0 - 1e-12);
       if (lb > sc.rcut2 || lb > d2min) continue;
+      if (sc.sure_box(fe_box_ub2(a.box + 6 * b, P))) return 1;
       const int q1 = min(32 * b + 32, a.npts);
       steps += q1 - 32 * b;
       for (int q = 32 * b; q < q1; ++q) {
@@ -473,6 +588,18 @@ __global__ void __launch_bounds__(FE_BUILD_THREADS) fe_build_kernel(const FeBuil
   }
 }
 
+// log2(x) for finite x > 0 and 2^y to about 1e-6 relative (float MUFU on the
+// mantissa, exact exponent arithmetic in double): starting points only.
+FE_DEV double fe_log2_approx(double x) {
+  int e;
+  const double m = frexp(x, &e);
+  return double(e) + double(__log2f(float(m)));
+}
+FE_DEV double fe_exp2_approx(double y) {
+  const double iy = floor(y);
+  return ldexp(double(exp2f(float(y - iy))), int(fmax(fmin(iy, 2000.0), -2000.0)));
+}
+
 // Radius beyond which sum_n b_n / r^(n+1) < tau (b_n >= 0): with u = 1/r the
 // sum is convex and increasing in u, so Newton's method started above the root
 // (at the smallest u where one term alone reaches tau) descends to it
@@ -481,10 +608,13 @@ __global__ void __launch_bounds__(FE_BUILD_THREADS) fe_build_kernel(const FeBuil
 FE_DEV double fe_route_radius(const double* b, int L, double tau) {
   double u = 1e300;
   bool any = false;
+  const double ltau = fe_log2_approx(tau);
   for (int n = 0; n <= L; ++n) {
     if (!(b[n] >= 0.0) || isinf(b[n])) return __longlong_as_double(0x7ff0000000000000LL);
     if (b[n] > 0.0) {
-      u = fmin(u, pow(tau / b[n], 1.0 / double(n + 1)));
+      // (tau / b_n)^(1/(n+1)), to ~1e-6, raised by 1e-4 so that the start is
+      // above every single term's root and so above the sum's
+      u = fmin(u, fe_exp2_approx((ltau - fe_log2_approx(b[n])) / double(n + 1)) * (1.0 + 1e-4));
       any = true;
     }
   }
@@ -610,6 +740,10 @@ __global__ void __launch_bounds__(128) fe_screen_pending_kernel(const FeBuildArg
         const int sbi = sb0 + __ffs(cm) - 1;
         cm &= cm - 1;
         if (fe_box_lb2(a.sbox + 6 * sbi, P) * (1.0 - 1e-12) > d2min) continue;
+        if (sc.sure_box(fe_box_ub2(a.sbox + 6 * sbi, P))) {
+          sure = true;
+          break;
+        }
         const int b = 32 * sbi + lane;
         bool bc = false;
         if (b < a.nbox) {
@@ -621,6 +755,10 @@ __global__ void __launch_bounds__(128) fe_screen_pending_kernel(const FeBuildArg
           const int bi = 32 * sbi + __ffs(bm) - 1;
           bm &= bm - 1;
           if (fe_box_lb2(a.box + 6 * bi, P) * (1.0 - 1e-12) > d2min) continue;
+          if (sc.sure_box(fe_box_ub2(a.box + 6 * bi, P))) {
+            sure = true;
+            break;
+          }
           const int q = 32 * bi + lane;
           double d2 = 1e300;
           if (q < a.npts) {
@@ -665,9 +803,10 @@ __global__ void fe_scatter_kernel(const double* __restrict__ stage, const long l
   reinterpret_cast<int*>(table + hdr->off_src)[base + dst] = swork[s];
 }
 
-// Per-class kept counts and the sum rule.  One block of 1024 threads: each
-// thread sums a fixed strided subset of slots, then a fixed-shape tree adds
-// the partial sums, so the result does not depend on scheduling.
+// Per-class kept counts and the sum rule.  One block of 1024 threads adds the
+// per-scan-block sums of the sum-rule terms (``srule``, fixed trees of
+// fe_scan_sums_kernel) in a fixed strided order and a fixed-shape tree, so the
+// result does not depend on scheduling.
 __global__ void __launch_bounds__(1024) fe_finalize_kernel(
     const long long* class_slot0, int nclass, long long nslot, const int* __restrict__ keep,
     const int* __restrict__ pos, const double* __restrict__ srule, unsigned char* table,
@@ -679,8 +818,10 @@ __global__ void __launch_bounds__(1024) fe_finalize_kernel(
     const long long a0 = class_slot0[t], a1 = class_slot0[t + 1];
     hdr->count[t] = a1 > a0 ? pos[a1 - 1] + keep[a1 - 1] - pos[a0] : 0;
   }
+  // srule holds one partial sum per scan block (fe_scan_sums_kernel)
+  const long long nb = (nslot + FE_SCAN_BLOCK - 1) / FE_SCAN_BLOCK;
   double s = 0.0;
-  for (long long q = t; q < nslot; q += 1024) s += srule[q];
+  for (long long q = t; q < nb; q += 1024) s += srule[q];
   red[t] = s;
   __syncthreads();
   for (int h = 512; h > 0; h >>= 1) {
@@ -697,42 +838,63 @@ __global__ void __launch_bounds__(1024) fe_finalize_kernel(
 
 // Exclusive scan of the keep flags in three deterministic passes:
 // per-block sums, a single-block scan of those sums, then per-block scans.
-#define FE_SCAN_BLOCK 1024
 
 __global__ void __launch_bounds__(FE_SCAN_BLOCK) fe_scan_sums_kernel(
-    const int* __restrict__ keep, long long n, int* __restrict__ bsum) {
+    const int* __restrict__ keep, long long n, int* __restrict__ bsum,
+    const double* __restrict__ srule = nullptr, double* __restrict__ bsr = nullptr) {
   __shared__ int red[FE_SCAN_BLOCK];
+  __shared__ double dred[FE_SCAN_BLOCK];
   const long long i = blockIdx.x * (long long)FE_SCAN_BLOCK + threadIdx.x;
   red[threadIdx.x] = i < n ? keep[i] : 0;
+  if (srule) dred[threadIdx.x] = i < n ? srule[i] : 0.0;
   __syncthreads();
   for (int h = FE_SCAN_BLOCK / 2; h > 0; h >>= 1) {
-    if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+    if (threadIdx.x < h) {
+      red[threadIdx.x] += red[threadIdx.x + h];
+      if (srule) dred[threadIdx.x] += dred[threadIdx.x + h];
+    }
     __syncthreads();
   }
-  if (threadIdx.x == 0) bsum[blockIdx.x] = red[0];
+  if (threadIdx.x == 0) {
+    bsum[blockIdx.x] = red[0];
+    if (srule) bsr[blockIdx.x] = dred[0];
+  }
 }
 
-// In-place exclusive scan of ``bsum`` (nb entries) by one block.
+// In-place exclusive scan of ``bsum`` (nb entries) by one block: every thread
+// sums its contiguous chunk, a shuffle scan over each warp and a scan of the
+// warp totals give the chunk offsets, then every thread writes its chunk.
 __global__ void __launch_bounds__(FE_SCAN_BLOCK) fe_scan_top_kernel(int* bsum, int nb) {
-  __shared__ int buf[FE_SCAN_BLOCK];
-  __shared__ int carry;
-  if (threadIdx.x == 0) carry = 0;
+  __shared__ int wsum[FE_SCAN_BLOCK / 32];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int chunk = (nb + FE_SCAN_BLOCK - 1) / FE_SCAN_BLOCK;
+  const int c0 = min(t * chunk, nb), c1 = min(c0 + chunk, nb);
+  int tot = 0;
+  for (int i = c0; i < c1; ++i) tot += bsum[i];
+  int inc = tot;                                   // inclusive scan within the warp
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += v;
+  }
+  if (lane == 31) wsum[w] = inc;
   __syncthreads();
-  for (int base = 0; base < nb; base += FE_SCAN_BLOCK) {
-    const int i = base + threadIdx.x;
-    const int v = i < nb ? bsum[i] : 0;
-    buf[threadIdx.x] = v;
-    __syncthreads();
-    for (int off = 1; off < FE_SCAN_BLOCK; off <<= 1) {   // Hillis-Steele inclusive scan
-      const int add = threadIdx.x >= off ? buf[threadIdx.x - off] : 0;
-      __syncthreads();
-      buf[threadIdx.x] += add;
-      __syncthreads();
+  if (w == 0) {
+    int v = lane < FE_SCAN_BLOCK / 32 ? wsum[lane] : 0;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += u;
     }
-    if (i < nb) bsum[i] = carry + buf[threadIdx.x] - v;
-    __syncthreads();
-    if (threadIdx.x == FE_SCAN_BLOCK - 1) carry += buf[FE_SCAN_BLOCK - 1];
-    __syncthreads();
+    if (lane < FE_SCAN_BLOCK / 32) wsum[lane] = x - v;     // exclusive warp offsets
+  }
+  __syncthreads();
+  int run = wsum[w] + inc - tot;                   // exclusive offset of this chunk
+  for (int i = c0; i < c1; ++i) {
+    const int v = bsum[i];
+    bsum[i] = run;
+    run += v;
   }
 }
 

@@ -226,7 +226,7 @@ struct fe_plan {
   size_t table_bytes = 0;
   size_t o_tab64[FE_NCLASS], o_tab32[FE_NCLASS], o_atoms = 0;
   size_t ws_stage = 0, ws_keep = 0, ws_pos = 0, ws_srule = 0, ws_swork = 0, ws_bsum = 0;
-  size_t ws_pending = 0, ws_npend = 0;
+  size_t ws_pending = 0, ws_npend = 0, ws_bsr = 0;
   long long nscan_blocks = 0;
   size_t ws_bytes = 0;
 };
@@ -388,6 +388,7 @@ int fe_plan_create(const fe_basis* b, fe_plan** out) {
   p->ws_npend = wput(sizeof(int));
   p->nscan_blocks = (p->nslot + FE_SCAN_BLOCK - 1) / FE_SCAN_BLOCK;
   p->ws_bsum = wput(size_t(p->nscan_blocks + 1) * sizeof(int));
+  p->ws_bsr = wput(size_t(p->nscan_blocks + 1) * sizeof(double));
   p->ws_bytes = std::max<size_t>(w, 256);
   *out = p;
   return FE_OK;
@@ -429,10 +430,32 @@ int fe_plan_upload(const fe_plan* p, void* d_plan, cudaStream_t st) {
   return FE_OK;
 }
 
+namespace {
+// Per-point part of the build workspace, after the plan's part: point-block
+// boxes, superboxes, the spatially sorted screen points, their cells, the
+// cell counters (FE_SORT_CELLS + 1) and the points' bounding box.
+struct ScreenWs {
+  size_t box, sbox, sorted, cell, count, bb, bytes;
+};
+ScreenWs screen_ws(size_t base, int n_pts) {
+  const size_t nbox = (size_t(n_pts) + 31) / 32, nsbox = (nbox + 31) / 32;
+  ScreenWs w{};
+  size_t o = base;
+  auto put = [&](size_t bytes) { const size_t at = o; o += align256(bytes); return at; };
+  w.box = put(nbox * 6 * sizeof(double));
+  w.sbox = put(nsbox * 6 * sizeof(double));
+  w.sorted = put(size_t(n_pts) * 3 * sizeof(double));
+  w.cell = put(size_t(n_pts) * sizeof(int));
+  w.count = put((FE_SORT_CELLS + 1) * sizeof(int));
+  w.bb = put(6 * FE_BBOX_BLOCKS * sizeof(double));
+  w.bytes = o;
+  return w;
+}
+}  // namespace
+
 size_t fe_build_ws_bytes(const fe_plan* p, int n_pts) {
   if (!p || n_pts < 0) return 0;
-  const size_t nbox = (size_t(n_pts) + 31) / 32, nsbox = (nbox + 31) / 32;
-  return p->ws_bytes + align256(nbox * 6 * sizeof(double)) + align256(nsbox * 6 * sizeof(double));
+  return screen_ws(p->ws_bytes, n_pts).bytes;
 }
 
 int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
@@ -483,12 +506,26 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
   a.npending = reinterpret_cast<int*>(wb + p->ws_npend);
   a.nbox = (n_pts + 31) / 32;
   a.nsbox = (a.nbox + 31) / 32;
-  double* box = reinterpret_cast<double*>(wb + p->ws_bytes);
-  double* sbox = reinterpret_cast<double*>(wb + p->ws_bytes + align256(size_t(a.nbox) * 6 * sizeof(double)));
+  const ScreenWs pw = screen_ws(p->ws_bytes, n_pts);
+  double* box = reinterpret_cast<double*>(wb + pw.box);
+  double* sbox = reinterpret_cast<double*>(wb + pw.sbox);
   a.box = box;
   a.sbox = sbox;
-  if (a.nbox > 0) {            // one warp per box and per superbox
-    fe_point_boxes_kernel<<<(a.nbox + 3) / 4, 128, 0, st>>>(d_pts, n_pts, box, a.nbox);
+  if (a.nbox > 0) {
+    // the screen's points bucketed by Morton cell, so that its boxes are compact
+    double* sorted = reinterpret_cast<double*>(wb + pw.sorted);
+    int* cell = reinterpret_cast<int*>(wb + pw.cell);
+    int* count = reinterpret_cast<int*>(wb + pw.count);
+    double* bb = reinterpret_cast<double*>(wb + pw.bb);
+    FE_CUDA(cudaMemsetAsync(count, 0, (FE_SORT_CELLS + 1) * sizeof(int), st));
+    fe_points_bbox_kernel<<<FE_BBOX_BLOCKS, 256, 0, st>>>(d_pts, n_pts, bb);
+    fe_points_count_kernel<<<(n_pts + 255) / 256, 256, 0, st>>>(d_pts, n_pts, bb, cell, count);
+    fe_scan_top_kernel<<<1, FE_SCAN_BLOCK, 0, st>>>(count, FE_SORT_CELLS);
+    fe_points_place_kernel<<<(n_pts + 255) / 256, 256, 0, st>>>(d_pts, n_pts, cell, count, sorted);
+    FE_CUDA(cudaGetLastError());
+    a.pts = sorted;
+    // one warp per box and per superbox
+    fe_point_boxes_kernel<<<(a.nbox + 3) / 4, 128, 0, st>>>(sorted, n_pts, box, a.nbox);
     fe_super_boxes_kernel<<<(a.nsbox + 3) / 4, 128, 0, st>>>(box, a.nbox, sbox, a.nsbox);
     FE_CUDA(cudaGetLastError());
   }
@@ -501,10 +538,12 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
     FE_CUDA(cudaGetLastError());
   }
   int* pos = reinterpret_cast<int*>(wb + p->ws_pos);
+  double* bsr = reinterpret_cast<double*>(wb + p->ws_bsr);
   if (p->nslot > 0) {
     int* bsum = reinterpret_cast<int*>(wb + p->ws_bsum);
     const unsigned nb = unsigned(p->nscan_blocks);
-    fe_scan_sums_kernel<<<nb, FE_SCAN_BLOCK, 0, st>>>(a.keep, p->nslot, bsum);
+    // the per-block keep counts, and the per-block sums of the sum-rule terms
+    fe_scan_sums_kernel<<<nb, FE_SCAN_BLOCK, 0, st>>>(a.keep, p->nslot, bsum, a.srule, bsr);
     fe_scan_top_kernel<<<1, FE_SCAN_BLOCK, 0, st>>>(bsum, int(nb));
     fe_scan_apply_kernel<<<nb, FE_SCAN_BLOCK, 0, st>>>(a.keep, p->nslot, bsum, pos);
     FE_CUDA(cudaGetLastError());
@@ -514,7 +553,7 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
         float(kTauDefault));
     FE_CUDA(cudaGetLastError());
   }
-  fe_finalize_kernel<<<1, 1024, 0, st>>>(a.class_slot0, FE_NCLASS, p->nslot, a.keep, pos, a.srule,
+  fe_finalize_kernel<<<1, 1024, 0, st>>>(a.class_slot0, FE_NCLASS, p->nslot, a.keep, pos, bsr,
                                          tb, float(kTauDefault));
   FE_CUDA(cudaGetLastError());
   return FE_OK;

@@ -557,6 +557,19 @@ def main() -> int:
     out.append("};")
     out.append("")
     # Boys grid
+    # e^(-i h) on the Boys grid's spacing up to T = 64, beyond every FP64
+    # asymptotic threshold (40-digit values): e^-T = e^(-i h) e^d, |d| <= h/2
+    import mpmath as mp
+    mp.mp.dps = 40
+    nexp = int(64.0 / GRID_H) + 1
+    out.append(f"#define FE_EXP_NROW {nexp}")
+    out.append("// e^(-i h), h = FE_BOYS_GRID_H, i = 0..FE_EXP_NROW-1")
+    out.append("__device__ const double fe_exp_grid[FE_EXP_NROW] = {")
+    vals = [float(mp.exp(-mp.mpf(i) * mp.mpf(GRID_H))) for i in range(nexp)]
+    for i in range(0, nexp, 6):
+        out.append("  " + ", ".join(repr(v) for v in vals[i:i + 6]) + ",")
+    out.append("};")
+    out.append("")
     rows = boys_grid()
     out.append(f"// F_n(i*h), i = 0..{len(rows) - 1}, n = 0..FE_BOYS_NTAB-1")
     out.append(f"#define FE_BOYS_NROW {len(rows)}")
