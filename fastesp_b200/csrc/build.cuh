@@ -391,8 +391,12 @@ struct FeScreen {
 };
 
 // One thread's screen with a budget of FE_SCREEN_BUDGET box/point tests:
-// 0 dropped, 1 kept, 2 undecided (the warp-parallel screen finishes it).
-FE_DEV int fe_screen_thread(const FeBuildArgs& a, const double (&P)[3], double KB, double reff) {
+// 0 dropped, 1 kept, 2 undecided (the warp-parallel screen finishes it).  Not
+// inlined: one copy serves the 25 (la, lb) instances of the build kernel, which
+// keeps that kernel's code small enough for the instruction cache.
+__device__ __noinline__ int fe_screen_thread(const FeBuildArgs& a, double px, double py,
+                                             double pz, double KB, double reff) {
+  const double P[3] = {px, py, pz};
   if (a.npts == 0 || a.tol <= 0.0) return 1;        // no points, or tol 0: every pair is kept
   const FeScreen sc(a, KB, reff);
   if (sc.none) return 0;
@@ -535,7 +539,7 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
   const double bound = pow(tp, -1.5) * bsum;
   const double reff = 1.6 * sqrt((L + 2.0) / p);
   const double KB = __dmul_rn(K, bound);
-  const int decided = fe_screen_thread(a, P, KB, reff);
+  const int decided = fe_screen_thread(a, P[0], P[1], P[2], KB, reff);
   if (decided == 0) return;
 
   // G_k = (2 pi / p) (2p)^m_k sum_t M0[k,t] etab[t], at record position fe_gpos_L[k]
