@@ -363,7 +363,7 @@ def run_ours(args):
     prof = ROOT / "profiles" / f"eval_{'mixed' if prec == 'mixed' else 'f64'}_frag54_30000.json"
     if prof.exists():
         traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
-    launches = 5 if prec == "mixed" else 3     # evaluator kernel instances + the reduction
+    launches = 6 if prec == "mixed" else 3     # evaluator kernel instances + the reduction
     line = {
         "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
