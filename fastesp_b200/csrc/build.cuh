@@ -391,11 +391,11 @@ struct FeScreen {
 };
 
 // One thread's screen with a budget of FE_SCREEN_BUDGET box/point tests:
-// 0 dropped, 1 kept, 2 undecided (the warp-parallel screen finishes it).  Not
-// inlined: one copy serves the 25 (la, lb) instances of the build kernel, which
-// keeps that kernel's code small enough for the instruction cache.
-__device__ __noinline__ int fe_screen_thread(const FeBuildArgs& a, double px, double py,
-                                             double pz, double KB, double reff) {
+// 0 dropped, 1 kept, 2 undecided (the warp-parallel screen finishes it).
+// (Not inlining it -- one copy for the 25 (la, lb) instances -- was measured:
+// no faster, and the call spilled more of the caller to local memory.)
+FE_DEV int fe_screen_thread(const FeBuildArgs& a, double px, double py, double pz, double KB,
+                            double reff) {
   const double P[3] = {px, py, pz};
   if (a.npts == 0 || a.tol <= 0.0) return 1;        // no points, or tol 0: every pair is kept
   const FeScreen sc(a, KB, reff);
