@@ -485,11 +485,23 @@ def run_extras(args, dev, flush, which=("grid", "adjoint", "batch")):
                                 device=dev)
         t54 = build_table(wfn, basis, P_d, pts54)
         w54 = torch.linspace(-1.0, 1.0, pts54.shape[0], dtype=torch.float64, device=dev)
+        t_fwd54 = _median_ms(lambda: t54.esp(pts54), 3, warm=1)
+        t_adj54 = _median_ms(lambda: t54.adjoint(pts54, w54), 3, warm=1)
+        t_dc54 = _median_ms(lambda: t54.adjoint(pts54, w54, density=False), 3, warm=1)
+        from fastesp_b200 import hermite as H
+        n54 = int(pts54.shape[0])
+        fl_field = float(sum(c * H.field_flops(L) for L, c in enumerate(t54.counts))) * n54
+        fl_mom = float(sum(c * H.eval_flops(L) for L, c in enumerate(t54.counts))) * n54
+        pk64 = peak_flops(torch, 1)
         out["adjoint"]["frag54_30000"] = {
-            "pairs": t54.n_pairs,
-            "forward_fp64_ms": _median_ms(lambda: t54.esp(pts54), 3, warm=1),
-            "adjoint_dP_dC_ms": _median_ms(lambda: t54.adjoint(pts54, w54), 3, warm=1),
-            "adjoint_dC_only_ms": _median_ms(lambda: t54.adjoint(pts54, w54, density=False), 3, warm=1)}
+            "pairs": t54.n_pairs, "forward_fp64_ms": t_fwd54, "adjoint_dP_dC_ms": t_adj54,
+            "adjoint_dC_only_ms": t_dc54,
+            "field_tflops": fl_field / (t_dc54 * 1e-3) / 1e12,
+            "field_frac_of_fp64_peak": fl_field / (t_dc54 * 1e-3) / pk64,
+            "density_part_tflops": fl_mom / max(1e-9, (t_adj54 - t_dc54) * 1e-3) / 1e12,
+            "density_part_frac_of_fp64_peak": fl_mom / max(1e-9, (t_adj54 - t_dc54) * 1e-3) / pk64,
+            "flops": "field: hermite.field_flops per (pair, point); density part (moments, "
+                     "pair back-transform, gather): hermite.eval_flops per (pair, point)"}
         del t54, pts54
     if "batch" in which:
         # batch: 64 uneven molecules

@@ -175,3 +175,12 @@ def build_flops(la: int, lb: int) -> int:
     nc = lambda l: (l + 1) * (l + 2) // 2  # noqa: E731
     nnz = sum(len(r) for r in class_terms(L)[1])
     return 3 * (la + 1) * (lb + 1) * (L + 1) * 4 + nc(la) * nc(lb) * (L + 1) ** 3 * 2 + 2 * nnz
+
+
+def field_flops(L: int) -> int:
+    """Algorithmic FLOPs of one (pair, point) of the potential-and-gradient
+    (field) evaluation: the potential's eval_flops, the companion sum
+    sum_k G_k R^a F_(m+1) (2 nt), the three monomial-derivative sums (6 nt),
+    the order L+1 of the Boys recursion (3), and d/dC = dS/dR - 2pR u plus
+    the three extra accumulations (18)."""
+    return eval_flops(L) + 8 * n_terms(L) + 21
