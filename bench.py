@@ -378,6 +378,7 @@ def run_ours(args):
         "mixed_over_fp64": ms_fp64 / ms_mixed,
         "mixed_error_vs_fp64": mixed_err,
         "table_build_ms": build_ms,
+        "table_build_warp_screen_pairs": int(tab.info.n_warp_screen),
         "e2e": e2e,
         "roofline": {"bound": "fp32" if prec == "mixed" else "fp64",
                      "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",

@@ -44,7 +44,7 @@ class FeSizes(C.Structure):
 class FeTableInfo(C.Structure):
     _fields_ = [("count", C.c_int * NCLASS), ("n_pairs", C.c_int), ("n_atoms", C.c_int),
                 ("sum_rule", C.c_double), ("tol", C.c_double), ("rule", C.c_int),
-                ("has_f32", C.c_int)]
+                ("has_f32", C.c_int), ("n_warp_screen", C.c_int)]
 
 
 class FeBatchMol(C.Structure):

@@ -2,13 +2,14 @@
 // and build_table / ESPEngine (fastesp/table.py:176-259, fastesp/esp.py:168-257).
 //
 // One thread per primitive pair.  Work items are grouped by the shell pair's
-// (la, lb) so that a block runs one template instance; a pair that survives
-// the screen is written to a fixed slot of its class's staging array (slots
-// are numbered in the reference's pair order), with a keep flag.  A thread
-// spends at most FE_SCREEN_BUDGET box/point tests on the screen; the pairs it
-// leaves undecided are finished by one warp each (fe_screen_pending_kernel).
-// A scan of the flags and a scatter kernel then compact every class in order
-// into the table, deriving the mixed-precision records on the way.
+// (la, lb), one launch per group (fe_build_kernel<la, lb>, the groups side by
+// side on forked streams); a pair that survives the screen is written to a
+// fixed slot of its class's staging array (slots are numbered in the
+// reference's pair order), with a keep flag.  A thread spends at most
+// FE_SCREEN_BUDGET box/point tests on the screen; the pairs it leaves
+// undecided are finished by one warp each (fe_screen_pending_kernel).
+// A scan of the flags, then one fe_records_kernel<L> per class, compact every
+// class in order into the table and derive its mixed-precision records.
 //
 // Per primitive pair (a = exponent of shell si, b = of sj):
 //   p = a + b, P = (aA + bB)/p, K = exp(-ab/p |A-B|^2)       (esp.py:226-230)
@@ -45,11 +46,6 @@ struct FeBuildArgs {
   const FeTask* tasks;
   const int* work_task;          // work item -> task
   const int* work_ij;            // work item -> (i << 16) | j
-  const int* grp_block0;         // first block of each (la, lb) group
-  const int* grp_code;           // la * 5 + lb
-  const int* grp_work0;          // first work item of each group
-  const int* grp_nwork;
-  int ngroup;
   int n_func;
   const double* dens;            // (n_func, n_func) Cartesian density
   const double* pts;             // (npts, 3)
@@ -62,18 +58,21 @@ struct FeBuildArgs {
   const long long* class_slot0;  // first global slot of class L in the staging arrays
   double* stage;                 // staging records, class L at stage_off[L] doubles
   const long long* stage_off;
-  int* keep;                     // per global slot: 0 dropped, 1 kept, 2 pending
+  int* keep;                     // per global slot: 0 dropped, 1 kept
   double* srule;                 // per global slot: K (pi/p)^1.5 etab[0]
   int* swork;                    // per global slot: its work item
-  int* pending;                  // slots whose screen ran past the search budget
+  int* pending;                  // slots whose screen ran past the thread's budget
   int* npending;                 // their count (capacity: the slot count)
 };
 
 // Box or point tests a thread spends on a pair's screen before it hands the
-// pair to the warp-parallel screen (fe_screen_pending_kernel).  Most pairs are
-// decided within it; the few that need the exact nearest distance over many
-// points would otherwise hold their whole warp (one thread per pair).
-#define FE_SCREEN_BUDGET 64
+// pair to the warp-parallel screen (fe_screen_warp).  Most pairs are decided
+// within it; the few that need the exact nearest distance over many points
+// would otherwise hold their whole warp (one thread per pair).  32 (about the
+// superbox sweep of 30000 points) measured faster than 64, 128 or 256.
+#ifndef FE_SCREEN_BUDGET
+#define FE_SCREEN_BUDGET 32
+#endif
 
 #define FE_SCAN_BLOCK 1024     // slots per block of the keep-flag scan
 
@@ -85,6 +84,19 @@ __constant__ signed char fe_cart[5][15][3] = {
    {0, 1, 2}, {0, 0, 3}},
   {{4, 0, 0}, {3, 1, 0}, {3, 0, 1}, {2, 2, 0}, {2, 1, 1}, {2, 0, 2}, {1, 3, 0}, {1, 2, 1},
    {1, 1, 2}, {1, 0, 3}, {0, 4, 0}, {0, 3, 1}, {0, 2, 2}, {0, 1, 3}, {0, 0, 4}}};
+
+// The exponent along axis k of Cartesian function idx of angular momentum l, in
+// the order of fe_cart (lx descending, then ly): a pure function, so inside
+// fully unrolled loops it folds to a constant.
+FE_DEV constexpr int fe_cart_exp(int l, int idx, int k) {
+  int i = 0;
+  for (int lx = l; lx >= 0; --lx)
+    for (int ly = l - lx; ly >= 0; --ly) {
+      if (i == idx) return k == 0 ? lx : (k == 1 ? ly : l - lx - ly);
+      ++i;
+    }
+  return 0;
+}
 
 __constant__ double fe_screen_mom[12] = {
   2.5066282746310002, 2.0, 1.5957691216057308, 4.0, 10.212920779565312, 33.63284766793385,
@@ -426,7 +438,7 @@ FE_DEV int fe_screen_thread(const FeBuildArgs& a, double px, double py, double p
 }
 
 template <int LA, int LB>
-FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
+FE_DEV long long fe_build_pair(const FeBuildArgs& a, int w) {
   constexpr int L = LA + LB;
   constexpr int NA = (LA + 1) * (LA + 2) / 2, NB = (LB + 1) * (LB + 2) / 2;
   constexpr int NTRI = (L + 1) * (L + 2) * (L + 3) / 6;
@@ -442,19 +454,20 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
   a.srule[slot] = 0.0;
   a.swork[slot] = w;
 
-  // density block of the shell pair (both orderings for si != sj)
-  double W[NA * NB];
+  // density block of the shell pair (both orderings for si != sj); read again
+  // where it is used (L1 hits) rather than held in a per-thread array, which
+  // would live in local memory
+  auto wdens = [&](int mu, int nu) {
+    double d = a.dens[size_t(A.fn0 + mu) * a.n_func + (B.fn0 + nu)];
+    if (tk.si != tk.sj) d += a.dens[size_t(B.fn0 + nu) * a.n_func + (A.fn0 + mu)];
+    return d;
+  };
   double wmax = 0.0;
 #pragma unroll
   for (int mu = 0; mu < NA; ++mu)
 #pragma unroll
-    for (int nu = 0; nu < NB; ++nu) {
-      double d = a.dens[size_t(A.fn0 + mu) * a.n_func + (B.fn0 + nu)];
-      if (tk.si != tk.sj) d += a.dens[size_t(B.fn0 + nu) * a.n_func + (A.fn0 + mu)];
-      W[mu * NB + nu] = d;
-      wmax = fmax(wmax, fabs(d));
-    }
-  if (!(wmax >= 1e-15)) return;
+    for (int nu = 0; nu < NB; ++nu) wmax = fmax(wmax, fabs(wdens(mu, nu)));
+  if (!(wmax >= 1e-15)) return -1;
 
   const double al = a.sexp[A.prim0 + ii], be = a.sexp[B.prim0 + jj];
   const double cc = a.scoef[A.prim0 + ii] * a.scoef[B.prim0 + jj];
@@ -466,8 +479,8 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
     ab2 += d * d;
   }
   const double K = exp(-(al * be) / p * ab2);
-  if (!(K >= 1e-30)) return;
-  if (a.rule == 1 && cc == 0.0) return;
+  if (!(K >= 1e-30)) return -1;
+  if (a.rule == 1 && cc == 0.0) return -1;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     P[k] = (al * A.c[k] + be * B.c[k]) / p;
@@ -483,12 +496,35 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
   double etab[NTRI];
 #pragma unroll
   for (int t = 0; t < NTRI; ++t) etab[t] = 0.0;
+  if constexpr (NA * NB <= 9) {
+    // small shell pairs: every loop fully unrolled, so every index is a
+    // compile-time constant and the E and etab arrays stay in registers
+#pragma unroll
+    for (int mu = 0; mu < NA; ++mu)
+#pragma unroll
+      for (int nu = 0; nu < NB; ++nu) {
+        const int ax = fe_cart_exp(LA, mu, 0), ay = fe_cart_exp(LA, mu, 1), az = fe_cart_exp(LA, mu, 2);
+        const int bx = fe_cart_exp(LB, nu, 0), by = fe_cart_exp(LB, nu, 1), bz = fe_cart_exp(LB, nu, 2);
+        const double wt = wdens(mu, nu) * cc;
+#pragma unroll
+        for (int tx = 0; tx <= ax + bx; ++tx) {
+          const double vx = wt * ex[ax][bx][tx];
+#pragma unroll
+          for (int ty = 0; ty <= ay + by; ++ty) {
+            const double vxy = vx * ey[ay][by][ty];
+            const int base = fe_tri<L>(tx, ty, 0);
+#pragma unroll
+            for (int tz = 0; tz <= az + bz; ++tz) etab[base + tz] += vxy * ez[az][bz][tz];
+          }
+        }
+      }
+  } else {
 #pragma unroll 1
   for (int mu = 0; mu < NA; ++mu) {
     const int ax = fe_cart[LA][mu][0], ay = fe_cart[LA][mu][1], az = fe_cart[LA][mu][2];
 #pragma unroll 1
     for (int nu = 0; nu < NB; ++nu) {
-      const double wt = W[mu * NB + nu] * cc;
+      const double wt = wdens(mu, nu) * cc;
       if (wt == 0.0) continue;
       const int bx = fe_cart[LB][nu][0], by = fe_cart[LB][nu][1], bz = fe_cart[LB][nu][2];
       for (int tx = 0; tx <= ax + bx; ++tx) {
@@ -501,6 +537,7 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
       }
     }
   }
+  }
   // sum rule: int rho_pair = K (pi/p)^1.5 etab[0]   (build_pairs.cpp:294-296)
   a.srule[slot] = K * pow(3.14159265358979323846 / p, 1.5) * etab[0];
 
@@ -509,16 +546,27 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
   const short* rc = fe_m0_col<L>();
   const float* rv = fe_m0_val<L>();
   const signed char* rm = fe_m0_m<L>();
+  // small pairs: the contraction sums as straight-line code (etab and the sums
+  // stay in registers); larger ones walk the sparse rows
+  constexpr bool kStraight = NA * NB <= 9;
+  static_assert(!kStraight || L <= FE_M0_UNROLL_LMAX, "small pair above the straight-line classes");
+  double gs[kStraight ? NT : 1];
+  if constexpr (kStraight) fe_m0_rows<L>(etab, gs);
   if (a.rule == 1) {
     // the C++ builder drops pairs whose G are all zero (build_pairs.cpp:309)
     bool anyg = false;
+    if constexpr (kStraight) {
+#pragma unroll
+      for (int k = 0; k < NT; ++k) anyg |= gs[k] != 0.0;
+    } else {
 #pragma unroll 1
-    for (int k = 0; k < NT && !anyg; ++k) {
-      double sk = 0.0;
-      for (int q = rp[k]; q < rp[k + 1]; ++q) sk += double(rv[q]) * etab[rc[q]];
-      anyg = sk != 0.0;
+      for (int k = 0; k < NT && !anyg; ++k) {
+        double sk = 0.0;
+        for (int q = rp[k]; q < rp[k + 1]; ++q) sk += double(rv[q]) * etab[rc[q]];
+        anyg = sk != 0.0;
+      }
     }
-    if (!anyg) return;
+    if (!anyg) return -1;
   }
 
   // screening bound (esp.py:251-254)
@@ -540,7 +588,7 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
   const double reff = 1.6 * sqrt((L + 2.0) / p);
   const double KB = __dmul_rn(K, bound);
   const int decided = fe_screen_thread(a, P[0], P[1], P[2], KB, reff);
-  if (decided == 0) return;
+  if (decided == 0) return -1;
 
   // G_k = (2 pi / p) (2p)^m_k sum_t M0[k,t] etab[t], at record position fe_gpos_L[k]
   const double cf = 2.0 * 3.14159265358979323846 / p;
@@ -549,12 +597,16 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
 #pragma unroll
   for (int m = 1; m <= L; ++m) pw[m] = pw[m - 1] * tp;
   double* rec = a.stage + a.stage_off[L] + (slot - a.class_slot0[L]) * REC;
-  const short* gpos = fe_gpos<L>();
+  if constexpr (kStraight) {
+    fe_g_store<L>(gs, pw, cf, rec + 6);
+  } else {
+    const short* gpos = fe_gpos<L>();
 #pragma unroll 1
-  for (int k = 0; k < NT; ++k) {
-    double sk = 0.0;
-    for (int q = rp[k]; q < rp[k + 1]; ++q) sk += double(rv[q]) * etab[rc[q]];
-    rec[6 + gpos[k]] = cf * pw[rm[k]] * sk;
+    for (int k = 0; k < NT; ++k) {
+      double sk = 0.0;
+      for (int q = rp[k]; q < rp[k + 1]; ++q) sk += double(rv[q]) * etab[rc[q]];
+      rec[6 + gpos[k]] = cf * pw[rm[k]] * sk;
+    }
   }
   rec[0] = p;
   rec[1] = P[0];
@@ -564,32 +616,128 @@ FE_DEV void fe_build_pair(const FeBuildArgs& a, int w) {
   rec[5] = KB;
 #pragma unroll
   for (int k = 6 + NT; k < REC; ++k) rec[k] = 0.0;
+  if (decided == 2) return slot;        // undecided: the block's warps finish it
   a.keep[slot] = decided;
-  if (decided == 2) {
+  return -1;
+}
+
+// The screen of one pair that its thread left undecided (fe_screen_thread ran
+// past its budget), by the 32 lanes of a warp that all pass the same slot:
+// superboxes across the lanes; then, one candidate superbox at a time, its
+// boxes across the lanes, each lane testing every point of its box if the
+// box's bounds leave it a candidate.  The decision is the serial search's:
+// it depends only on whether some candidate box lies wholly within the keep
+// radius (sure_box) and on the minimum squared distance over the points
+// within rcut, which the box bounds only prune -- a box whose lower bound
+// exceeds the minimum found so far holds no point that lowers it.  The lanes
+// agree on d2min after each superbox (a shuffle reduction), so the decision
+// comes back in every lane.
+FE_DEV bool fe_screen_warp(const FeBuildArgs& a, long long slot, int L, int lane) {
+  const double* rec = a.stage + a.stage_off[L] + (slot - a.class_slot0[L]) * fe_c_rec64[L];
+  const double P[3] = {rec[1], rec[2], rec[3]};
+  const FeScreen sc(a, rec[5], 1.6 * sqrt((L + 2.0) / rec[0]));
+  double d2min = 1e300;
+  bool sure = sc.none;                        // (cannot happen: its thread searched)
+  for (int sb0 = 0; sb0 < a.nsbox && !sure; sb0 += 32) {
+    bool cand = false;
+    if (sb0 + lane < a.nsbox) {
+      const double ls = fe_box_lb2(a.sbox + 6 * (sb0 + lane), P) * (1.0 - 1e-12);
+      cand = ls <= sc.rcut2 && ls <= d2min;
+    }
+    unsigned cm = __ballot_sync(0xffffffffu, cand);
+    while (cm && !sure) {
+      const int sbi = sb0 + __ffs(cm) - 1;
+      cm &= cm - 1;
+      if (fe_box_lb2(a.sbox + 6 * sbi, P) * (1.0 - 1e-12) > d2min) continue;
+      if (sc.sure_box(fe_box_ub2(a.sbox + 6 * sbi, P))) {
+        sure = true;
+        break;
+      }
+      const int b = 32 * sbi + lane;
+      bool bsure = false;
+      double dl = 1e300;
+      if (b < a.nbox) {
+        const double lb = fe_box_lb2(a.box + 6 * b, P) * (1.0 - 1e-12);
+        if (lb <= sc.rcut2 && lb <= d2min) {
+          if (sc.sure_box(fe_box_ub2(a.box + 6 * b, P))) {
+            bsure = true;
+          } else {
+            const int q1 = min(32 * b + 32, a.npts);
+#pragma unroll 8
+            for (int q = 32 * b; q < q1; ++q) {
+              const double d2 = FeScreen::dist2(a.pts + 3 * q, P);
+              if (d2 <= sc.rcut2) dl = fmin(dl, d2);
+            }
+          }
+        }
+      }
+      if (__any_sync(0xffffffffu, bsure)) {
+        sure = true;
+        break;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) dl = fmin(dl, __shfl_xor_sync(0xffffffffu, dl, o));
+      d2min = fmin(d2min, dl);
+      sure = d2min < 1e300 && sc.sure_keep(d2min);
+    }
+  }
+  return sure || sc.keep_exact(d2min);
+}
+
+#define FE_BUILD_THREADS 128
+
+// One launch per (la, lb) group of work items (all primitive pairs of the
+// shell pairs with these angular momenta): each group's code gets its own
+// register allocation -- a single kernel over every group took the largest
+// group's registers and spilled -- and the groups' launches run side by side
+// on forked streams, so the long-running high-(la, lb) threads overlap the
+// many light ones.
+//
+// A pair its thread leaves undecided goes to the pending list, which
+// fe_screen_pending_kernel finishes after every group (finishing them inside
+// the group's blocks was measured slower: the searching warps hold their
+// blocks, and the long heavy-group blocks grow longer still).
+template <int LA, int LB>
+__global__ void __launch_bounds__(FE_BUILD_THREADS) fe_build_kernel(const FeBuildArgs a,
+                                                                    int work0, int nwork) {
+  const int w = int(blockIdx.x) * FE_BUILD_THREADS + int(threadIdx.x);
+  if (w >= nwork) return;
+  const long long slot = fe_build_pair<LA, LB>(a, work0 + w);
+  if (slot >= 0) {
     const int at = atomicAdd(a.npending, 1);
     if (at < int(a.class_slot0[FE_NCLASS])) a.pending[at] = int(slot);
     else fe_flag(FE_ST_OVERFLOW);
   }
 }
 
-#define FE_BUILD_THREADS 128
-
-__global__ void __launch_bounds__(FE_BUILD_THREADS) fe_build_kernel(const FeBuildArgs a) {
-  int g = 0;
-  while (g + 1 < a.ngroup && int(blockIdx.x) >= a.grp_block0[g + 1]) ++g;
-  const int w = (blockIdx.x - a.grp_block0[g]) * FE_BUILD_THREADS + threadIdx.x;
-  if (w >= a.grp_nwork[g]) return;
-  const int wi = a.grp_work0[g] + w;
-  switch (a.grp_code[g]) {
-#define FE_CASE(la, lb) case la * 5 + lb: fe_build_pair<la, lb>(a, wi); break;
-    FE_CASE(0, 0) FE_CASE(0, 1) FE_CASE(0, 2) FE_CASE(0, 3) FE_CASE(0, 4)
-    FE_CASE(1, 0) FE_CASE(1, 1) FE_CASE(1, 2) FE_CASE(1, 3) FE_CASE(1, 4)
-    FE_CASE(2, 0) FE_CASE(2, 1) FE_CASE(2, 2) FE_CASE(2, 3) FE_CASE(2, 4)
-    FE_CASE(3, 0) FE_CASE(3, 1) FE_CASE(3, 2) FE_CASE(3, 3) FE_CASE(3, 4)
-    FE_CASE(4, 0) FE_CASE(4, 1) FE_CASE(4, 2) FE_CASE(4, 3) FE_CASE(4, 4)
-#undef FE_CASE
-    default: fe_flag(FE_ST_BADCLASS); break;
+// The pending pairs, one warp each.
+__global__ void __launch_bounds__(128) fe_screen_pending_kernel(const FeBuildArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int warp = int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nwarp = int((gridDim.x * blockDim.x) >> 5);
+  const int np = min(*a.npending, int(a.class_slot0[FE_NCLASS]));
+  for (int i = warp; i < np; i += nwarp) {
+    const long long slot = a.pending[i];
+    int L = 0;
+    while (L + 1 < FE_NCLASS && slot >= a.class_slot0[L + 1]) ++L;
+    const bool keep = fe_screen_warp(a, slot, L, lane);
+    if (lane == 0) a.keep[slot] = keep ? 1 : 0;
   }
+}
+
+using FeBuildKernel = void (*)(const FeBuildArgs, int, int);
+
+// The group kernel of code la * 5 + lb.
+inline FeBuildKernel fe_build_kernel_for(int code) {
+#define FE_K(la, lb) fe_build_kernel<la, lb>,
+  static const FeBuildKernel k[25] = {
+    FE_K(0, 0) FE_K(0, 1) FE_K(0, 2) FE_K(0, 3) FE_K(0, 4)
+    FE_K(1, 0) FE_K(1, 1) FE_K(1, 2) FE_K(1, 3) FE_K(1, 4)
+    FE_K(2, 0) FE_K(2, 1) FE_K(2, 2) FE_K(2, 3) FE_K(2, 4)
+    FE_K(3, 0) FE_K(3, 1) FE_K(3, 2) FE_K(3, 3) FE_K(3, 4)
+    FE_K(4, 0) FE_K(4, 1) FE_K(4, 2) FE_K(4, 3) FE_K(4, 4)};
+#undef FE_K
+  return code >= 0 && code < 25 ? k[code] : nullptr;
 }
 
 // log2(x) for finite x > 0 and 2^y to about 1e-6 relative (float MUFU on the
@@ -609,10 +757,12 @@ FE_DEV double fe_exp2_approx(double y) {
 // (at the smallest u where one term alone reaches tau) descends to it
 // monotonically.  0 when every b_n is 0 (never routed); +inf when a b_n is not
 // finite.  Widened by 1e-6 relative so the radius is never below the exact one.
-FE_DEV double fe_route_radius(const double* b, int L, double tau) {
+template <int L>
+FE_DEV double fe_route_radius(const double (&b)[L + 1], double tau) {
   double u = 1e300;
   bool any = false;
   const double ltau = fe_log2_approx(tau);
+#pragma unroll
   for (int n = 0; n <= L; ++n) {
     if (!(b[n] >= 0.0) || isinf(b[n])) return __longlong_as_double(0x7ff0000000000000LL);
     if (b[n] > 0.0) {
@@ -625,6 +775,7 @@ FE_DEV double fe_route_radius(const double* b, int L, double tau) {
   if (!any) return 0.0;
   for (int it = 0; it < 100; ++it) {
     double g = 0.0, dg = 0.0;                 // g = sum b_n u^n and g'(u), Horner
+#pragma unroll
     for (int n = L; n >= 0; --n) {
       dg = fma(dg, u, g);
       g = fma(g, u, b[n]);
@@ -637,19 +788,13 @@ FE_DEV double fe_route_radius(const double* b, int L, double tau) {
   return (1.0 + 1e-6) / u;
 }
 
-// FP32 asymptotic Boys thresholds by class, for runtime indexing.
-__constant__ float fe_c_boys32_asym_T[FE_NCLASS] = {
-  fe_boys32_asym_T[0], fe_boys32_asym_T[1], fe_boys32_asym_T[2], fe_boys32_asym_T[3],
-  fe_boys32_asym_T[4], fe_boys32_asym_T[5], fe_boys32_asym_T[6], fe_boys32_asym_T[7],
-  fe_boys32_asym_T[8]};
-
 // The mixed-precision record of one FP64 record ``r`` of class L (layout in
 // table.cuh): coefficients c_k = K G_k s_m p^-(m+1/2) and the routing-bound
 // coefficients formed in FP64, then rounded to float once.  ``tau_fast`` is
 // the routing threshold the far radius is computed for.
-FE_DEV void fe_f32_record(const double* __restrict__ r, float* __restrict__ o, int L,
-                          float tau_fast) {
-  const int R32 = fe_c_rec32[L], NT = fe_c_nterm[L];
+template <int L>
+FE_DEV void fe_f32_record(const double* __restrict__ r, float* __restrict__ o, float tau_fast) {
+  constexpr int R32 = fe_class_rec32[L], NT = fe_class_nterm[L];
   auto split = [](double v, float& hi, float& lo) {
     hi = float(v);
     lo = float(v - double(hi));
@@ -664,26 +809,23 @@ FE_DEV void fe_f32_record(const double* __restrict__ r, float* __restrict__ o, i
   // s_m = (sqrt(pi)/2) (2m-1)!!/2^m (the FP32 Boys vector is F_m / s_m,
   // boys.cuh) and p^-(m+1/2): with both folded in, F_m of an asymptotic
   // point is 1/|R|^(2m+1) exactly
-  double sm[FE_NCLASS], pm[FE_NCLASS];
+  double sm[L + 1], pm[L + 1];
+  const double ip = 1.0 / p;
   sm[0] = FE_SQRT_PI_2;
   pm[0] = 1.0 / sqrt(p);
+#pragma unroll
   for (int m = 1; m <= L; ++m) {
     sm[m] = sm[m - 1] * (0.5 * double(2 * m - 1));
-    pm[m] = pm[m - 1] / p;
+    pm[m] = pm[m - 1] * ip;
   }
-  const int c0 = fe_route_off[L];
-  for (int k = 0; k < NT; ++k) {
-    const int m = fe_route_nm[c0 + k] >> 4;
-    o[12 + 2 * k] = o[13 + 2 * k] = float(K * r[6 + k] * sm[m] * pm[m]);
-  }
-  // routing bound: K sum_k |G_k R^a F_m| <= sum_n b_n / |R|^(n+1) with
-  // b_n = K sum_{k: 2m - |a| = n} |G_k| c_k p^-(m + 1/2); rounded up to float
-  double b[FE_NCLASS];
+  // coefficient pairs, and the routing bound: K sum_k |G_k R^a F_m| <=
+  // sum_n b_n / |R|^(n+1) with b_n = K sum_{k: 2m - |a| = n} |G_k| c_k
+  // p^-(m + 1/2), rounded up to float
+  double b[L + 1];
+#pragma unroll
   for (int q = 0; q <= L; ++q) b[q] = 0.0;
-  for (int k = 0; k < NT; ++k) {
-    const unsigned nm = fe_route_nm[c0 + k];
-    b[nm & 15u] += fabs(r[6 + k]) * fe_route_c[c0 + k] * pm[nm >> 4];
-  }
+  fe_f32_terms<L>(r + 6, K, sm, pm, o + 12, b);
+#pragma unroll
   for (int q = 0; q <= L; ++q) {
     o[12 + 2 * NT + q] = __double2float_ru(K * b[q]);
     b[q] = double(o[12 + 2 * NT + q]);
@@ -691,130 +833,124 @@ FE_DEV void fe_f32_record(const double* __restrict__ r, float* __restrict__ o, i
   // far radius: the FP32 Boys vector is asymptotic (T = p r^2 beyond the
   // class's FP32 threshold) and the bound (with the stored, rounded-up b_n)
   // is below tau_fast
-  const double rt = fe_route_radius(b, L, double(tau_fast));
-  const double ra2 = double(fe_c_boys32_asym_T[L]) / p * (1.0 + 1e-6);
+  const double rt = fe_route_radius<L>(b, double(tau_fast));
+  constexpr double tas = double(fe_boys32_asym_T[L]);
+  const double ra2 = tas * ip * (1.0 + 1e-6);
   o[8] = __double2float_ru(fmax(ra2, rt * rt));
+#pragma unroll
   for (int k = 13 + 2 * NT + L; k < R32; ++k) o[k] = 0.0f;
 }
 
-// Mixed-precision records of a table whose FP64 records are in place (an
-// imported table): fe_f32_record per record.
-__global__ void fe_make_f32_kernel(unsigned char* table, float tau_fast) {
+// Records per block of fe_records_kernel<L>: the tile's FP64 and FP32 records
+// are both staged in shared memory (at most 78 KB, class 8).
+__host__ __device__ constexpr int fe_records_tile_of(int L) {
+  return L <= 3 ? 128 : (L == 4 ? 64 : (L == 5 ? 32 : 16));
+}
+template <int L>
+constexpr int fe_records_tile() { return fe_records_tile_of(L); }
+
+// Shared-memory row strides of the staged records, odd so that the thread of
+// each record reads and writes its own row without bank conflicts.
+template <int L>
+constexpr int fe_records_smem_bytes() {
+  return fe_records_tile<L>() * ((fe_class_rec64[L] + 1) * 8 + (fe_class_rec32[L] + 1) * 4);
+}
+
+// The table's records of class L, a tile of consecutive records per block:
+//
+// * build (``keep`` set): the tile is a range of the class's staging slots.
+//   The kept slots' FP64 records move, in slot order, to their final rows
+//   (``pos``, the exclusive scan of ``keep`` over all slots, gives the first
+//   row of the tile), together with each one's work item in the table's
+//   source section; then their mixed-precision records are derived.
+// * imported table (``keep`` null): the FP64 records are in place and the
+//   mixed-precision records of rows 0 .. count-1 are derived.
+//
+// Global loads and stores are coalesced (consecutive threads, consecutive
+// words); each record's FP32 derivation runs in one thread on the staged copy.
+template <int L>
+__global__ void __launch_bounds__(128) fe_records_kernel(
+    const double* __restrict__ stage, const int* __restrict__ keep, const int* __restrict__ pos,
+    const int* __restrict__ swork, int nslot, unsigned char* table, float tau_fast) {
+  constexpr int T = fe_records_tile<L>();
+  constexpr int R64 = fe_class_rec64[L], R32 = fe_class_rec32[L];
+  constexpr int S64 = R64 + 1, S32 = R32 + 1;
+  extern __shared__ double fe_rec_smem[];
+  double* in = fe_rec_smem;                                        // T x S64
+  float* out = reinterpret_cast<float*>(fe_rec_smem + T * S64);    // T x S32
+  __shared__ int src[T];
+  __shared__ int wsum[4];
   FeTableHdr* hdr = reinterpret_cast<FeTableHdr*>(table);
-  const int L = blockIdx.y;
-  const int n = hdr->count[L];
-  const double* src = reinterpret_cast<const double*>(table + hdr->off64[L]);
-  float* dst = reinterpret_cast<float*>(table + hdr->off32[L]);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    fe_f32_record(src + size_t(i) * fe_c_rec64[L], dst + size_t(i) * fe_c_rec32[L], L, tau_fast);
-  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+  double* t64 = reinterpret_cast<double*>(table + hdr->off64[L]);
+  float* t32 = reinterpret_cast<float*>(table + hdr->off32[L]);
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int n_all = keep ? nslot : min(hdr->count[L], hdr->cap[L]);
+  for (int s0 = int(blockIdx.x) * T; s0 < n_all; s0 += int(gridDim.x) * T) {
+    const int n = min(T, n_all - s0);
+    int nk = n, d0 = s0;
+    if (keep) {
+      // kept slots of the tile, in order: warp ballots, then the warps' prefix
+      const bool k = tid < n && keep[s0 + tid] != 0;
+      const unsigned bal = __ballot_sync(0xffffffffu, k);
+      if (lane == 0) wsum[wid] = __popc(bal);
+      __syncthreads();
+      int before = 0;
+      nk = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        before += q < wid ? wsum[q] : 0;
+        nk += wsum[q];
+      }
+      if (k) src[before + __popc(bal & ((1u << lane) - 1u))] = tid;
+      d0 = pos[s0] - pos[0];
+      if (d0 + nk > hdr->cap[L]) {
+        if (tid == 0) fe_flag(FE_ST_OVERFLOW);
+        nk = max(0, hdr->cap[L] - d0);
+      }
+      __syncthreads();
+      // FP64 records to their rows (and to shared memory), work items to the
+      // source section
+      for (int e = tid; e < nk * R64; e += 128) {
+        const int r = e / R64, c = e - r * R64;
+        const double v = stage[size_t(s0 + src[r]) * R64 + c];
+        in[r * S64 + c] = v;
+        t64[size_t(d0) * R64 + e] = v;
+      }
+      if (tid < nk) {
+        long long base = 0;
+        for (int l = 0; l < L; ++l) base += hdr->cap[l];
+        reinterpret_cast<int*>(table + hdr->off_src)[base + d0 + tid] = swork[s0 + src[tid]];
+      }
+    } else {
+      for (int e = tid; e < n * R64; e += 128) {
+        const int r = e / R64, c = e - r * R64;
+        in[r * S64 + c] = t64[size_t(s0) * R64 + e];
+      }
+    }
+    __syncthreads();
+    if (tid < nk) fe_f32_record<L>(in + tid * S64, out + tid * S32, tau_fast);
+    __syncthreads();
+    for (int e = tid; e < nk * R32; e += 128) {
+      const int r = e / R32, c = e - r * R32;
+      t32[size_t(d0) * R32 + e] = out[r * S32 + c];
+    }
+    __syncthreads();
+  }
+  if (!keep && L == 0 && blockIdx.x == 0 && tid == 0) {
     hdr->has32 = 1;
     hdr->tau_fast = tau_fast;
   }
 }
 
-// One warp per pair that its thread left undecided (fe_screen_thread ran past
-// its budget): the same decision, searched by 32 lanes -- superboxes across
-// the lanes, then the boxes of each candidate superbox, then the points of
-// each candidate box -- in the serial search's order.  d2min, the minimum over
-// the points within rcut found so far, is the same in every lane (a shuffle
-// reduction), so the pruning and the final decision are the serial search's.
-__global__ void __launch_bounds__(128) fe_screen_pending_kernel(const FeBuildArgs a) {
-  const int lane = threadIdx.x & 31;
-  const int warp = int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int nwarp = int((gridDim.x * blockDim.x) >> 5);
-  const int np = min(*a.npending, int(a.class_slot0[FE_NCLASS]));
-  for (int i = warp; i < np; i += nwarp) {
-    const long long slot = a.pending[i];
-    int L = 0;
-    while (L + 1 < FE_NCLASS && slot >= a.class_slot0[L + 1]) ++L;
-    const double* rec = a.stage + a.stage_off[L] + (slot - a.class_slot0[L]) * fe_c_rec64[L];
-    const double P[3] = {rec[1], rec[2], rec[3]};
-    const FeScreen sc(a, rec[5], 1.6 * sqrt((L + 2.0) / rec[0]));
-    double d2min = 1e300;
-    bool sure = sc.none;                      // (cannot happen: its thread searched)
-    for (int sb0 = 0; sb0 < a.nsbox && !sure; sb0 += 32) {
-      bool cand = false;
-      if (sb0 + lane < a.nsbox) {
-        const double ls = fe_box_lb2(a.sbox + 6 * (sb0 + lane), P) * (1.0 - 1e-12);
-        cand = ls <= sc.rcut2 && ls <= d2min;
-      }
-      unsigned cm = __ballot_sync(0xffffffffu, cand);
-      while (cm && !sure) {
-        const int sbi = sb0 + __ffs(cm) - 1;
-        cm &= cm - 1;
-        if (fe_box_lb2(a.sbox + 6 * sbi, P) * (1.0 - 1e-12) > d2min) continue;
-        if (sc.sure_box(fe_box_ub2(a.sbox + 6 * sbi, P))) {
-          sure = true;
-          break;
-        }
-        const int b = 32 * sbi + lane;
-        bool bc = false;
-        if (b < a.nbox) {
-          const double lb = fe_box_lb2(a.box + 6 * b, P) * (1.0 - 1e-12);
-          bc = lb <= sc.rcut2 && lb <= d2min;
-        }
-        unsigned bm = __ballot_sync(0xffffffffu, bc);
-        while (bm && !sure) {
-          const int bi = 32 * sbi + __ffs(bm) - 1;
-          bm &= bm - 1;
-          if (fe_box_lb2(a.box + 6 * bi, P) * (1.0 - 1e-12) > d2min) continue;
-          if (sc.sure_box(fe_box_ub2(a.box + 6 * bi, P))) {
-            sure = true;
-            break;
-          }
-          const int q = 32 * bi + lane;
-          double d2 = 1e300;
-          if (q < a.npts) {
-            d2 = FeScreen::dist2(a.pts + 3 * q, P);
-            if (!(d2 <= sc.rcut2)) d2 = 1e300;
-          }
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) d2 = fmin(d2, __shfl_xor_sync(0xffffffffu, d2, o));
-          d2min = fmin(d2min, d2);
-          sure = d2min < 1e300 && sc.sure_keep(d2min);
-        }
-      }
-    }
-    if (lane == 0) a.keep[slot] = (sure || sc.keep_exact(d2min)) ? 1 : 0;
-  }
-}
-
-// Move kept staging records of every class, in slot order, into the table,
-// derive their mixed-precision records, and record each one's work item in
-// the table's source section.
-// ``pos`` is the exclusive scan of ``keep`` over all global slots.
-__global__ void fe_scatter_kernel(const double* __restrict__ stage, const long long* stage_off,
-                                  const long long* class_slot0, int nclass,
-                                  const int* __restrict__ keep, const int* __restrict__ pos,
-                                  const int* __restrict__ swork, long long nslot,
-                                  unsigned char* table, float tau_fast) {
-  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (s >= nslot || !keep[s]) return;
-  int L = 0;
-  while (L + 1 < nclass && s >= class_slot0[L + 1]) ++L;
-  const FeTableHdr* hdr = reinterpret_cast<const FeTableHdr*>(table);
-  const int dst = pos[s] - pos[class_slot0[L]];
-  if (dst >= hdr->cap[L]) { fe_flag(FE_ST_OVERFLOW); return; }
-  const int R = fe_c_rec64[L];
-  const double* src = stage + stage_off[L] + (s - class_slot0[L]) * R;
-  double* out = reinterpret_cast<double*>(table + hdr->off64[L]) + size_t(dst) * R;
-  for (int k = 0; k < R; ++k) out[k] = src[k];
-  fe_f32_record(src, reinterpret_cast<float*>(table + hdr->off32[L]) + size_t(dst) * fe_c_rec32[L],
-                L, tau_fast);
-  long long base = 0;
-  for (int l = 0; l < L; ++l) base += hdr->cap[l];
-  reinterpret_cast<int*>(table + hdr->off_src)[base + dst] = swork[s];
-}
-
 // Per-class kept counts and the sum rule.  One block of 1024 threads adds the
 // per-scan-block sums of the sum-rule terms (``srule``, fixed trees of
 // fe_scan_sums_kernel) in a fixed strided order and a fixed-shape tree, so the
-// result does not depend on scheduling.
+// result does not depend on scheduling.  The mixed-precision records
+// (fe_records_kernel) were derived for the routing threshold ``tau_fast``.
 __global__ void __launch_bounds__(1024) fe_finalize_kernel(
     const long long* class_slot0, int nclass, long long nslot, const int* __restrict__ keep,
-    const int* __restrict__ pos, const double* __restrict__ srule, unsigned char* table,
-    float tau_fast) {
+    const int* __restrict__ pos, const double* __restrict__ srule, const int* __restrict__ npending,
+    unsigned char* table, float tau_fast) {
   __shared__ double red[1024];
   FeTableHdr* hdr = reinterpret_cast<FeTableHdr*>(table);
   const int t = threadIdx.x;
@@ -835,8 +971,9 @@ __global__ void __launch_bounds__(1024) fe_finalize_kernel(
   if (t == 0) {
     hdr->sum_rule = red[0];
     hdr->has_src = 1;
-    hdr->has32 = 1;                      // the scatter wrote the FP32 records
+    hdr->has32 = 1;
     hdr->tau_fast = tau_fast;
+    hdr->n_warp_screen = npending ? *npending : 0;
   }
 }
 

@@ -69,6 +69,122 @@ int sm_count() {
   return n > 0 ? n : 148;
 }
 
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// ID of the calling thread's current context (0 when none is current), from
+// the driver's entry points as the runtime hands them out (no link to libcuda).
+unsigned long long current_ctx_id() {
+  static CtxGetCurrentFn get_cur = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_cur = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+  });
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_cur || !get_id || get_cur(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Side streams of the table build, per device: the build's (la, lb) group
+// launches fork from the caller's stream onto these and join back through
+// events, so the groups run side by side and every later launch on the
+// caller's stream waits for all of them.  Created on first use; a device reset
+// (a new context ID) makes them be created again.  The mutex is held from the
+// fork to the join, so concurrent builds on one device take turns on them.
+#define FE_SIDE_STREAMS 8
+#define FE_SIDE_MAX_DEVICES 128
+struct SideStreams {
+  cudaStream_t s[FE_SIDE_STREAMS] = {};
+  cudaEvent_t fork = nullptr, join[FE_SIDE_STREAMS] = {};
+  unsigned long long ctx_id = 0;
+};
+std::mutex g_side_mu;
+SideStreams g_side[FE_SIDE_MAX_DEVICES];
+
+int side_streams(SideStreams** out) {
+  int dev = 0;
+  FE_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= FE_SIDE_MAX_DEVICES)
+    return fail(FE_ERR_UNSUPPORTED, "table build: device ordinal %d too large", dev);
+  SideStreams& ss = g_side[dev];
+  const unsigned long long id = current_ctx_id();
+  if (!ss.fork || id == 0 || id != ss.ctx_id) {
+    // handles of a replaced context are not destroyed: they died with it
+    ss = SideStreams{};
+    for (int i = 0; i < FE_SIDE_STREAMS; ++i) {
+      FE_CUDA(cudaStreamCreateWithFlags(&ss.s[i], cudaStreamNonBlocking));
+      FE_CUDA(cudaEventCreateWithFlags(&ss.join[i], cudaEventDisableTiming));
+    }
+    FE_CUDA(cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming));
+    ss.ctx_id = current_ctx_id();
+  }
+  *out = &ss;
+  return FE_OK;
+}
+
+// Run launch(i, stream) for i = 0..n-1 side by side: item i goes to the
+// caller's stream (i % (k + 1) == 0) or side stream i % (k + 1) - 1, k the
+// side streams used; the side streams start after the work already on ``st``
+// and every later launch on ``st`` waits for them.  The side streams are
+// joined even when a launch fails.
+template <typename F>
+int fork_join(int n, cudaStream_t st, F&& launch) {
+  if (n <= 0) return FE_OK;
+  std::lock_guard<std::mutex> lock(g_side_mu);
+  SideStreams* ss = nullptr;
+  int rc = side_streams(&ss);
+  if (rc != FE_OK) return rc;
+  const int nside = std::min(n - 1, FE_SIDE_STREAMS);
+  if (nside > 0) FE_CUDA(cudaEventRecord(ss->fork, st));
+  for (int i = 0; i < nside; ++i) FE_CUDA(cudaStreamWaitEvent(ss->s[i], ss->fork, 0));
+  for (int i = 0; i < n && rc == FE_OK; ++i) {
+    const int q = i % (nside + 1);
+    rc = launch(i, q == 0 ? st : ss->s[q - 1]);
+  }
+  for (int i = 0; i < nside; ++i) {
+    FE_CUDA(cudaEventRecord(ss->join[i], ss->s[i]));
+    FE_CUDA(cudaStreamWaitEvent(st, ss->join[i], 0));
+  }
+  return rc;
+}
+
+// fe_records_kernel<L> on ``st``: the build's compaction of class L (``keep``
+// set; stage, keep, pos and swork are the class's slices, nslot its slot
+// count) or, for an imported table, the derivation of its FP32 records.
+template <int L>
+int launch_records_l(const double* stage, const int* keep, const int* pos, const int* swork,
+                     int nslot, unsigned char* table, unsigned grid, cudaStream_t st) {
+  constexpr int smem = fe_records_smem_bytes<L>();
+  FE_CUDA(cudaFuncSetAttribute(fe_records_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               smem));
+  fe_records_kernel<L><<<grid, 128, smem, st>>>(stage, keep, pos, swork, nslot, table,
+                                                float(kTauDefault));
+  FE_CUDA(cudaGetLastError());
+  return FE_OK;
+}
+
+int launch_records(int L, const double* stage, const int* keep, const int* pos,
+                   const int* swork, int nslot, unsigned char* table, unsigned grid,
+                   cudaStream_t st) {
+  switch (L) {
+#define FE_R(l) case l: return launch_records_l<l>(stage, keep, pos, swork, nslot, table, grid, st);
+    FE_R(0) FE_R(1) FE_R(2) FE_R(3) FE_R(4) FE_R(5) FE_R(6) FE_R(7) FE_R(8)
+#undef FE_R
+    default: return fail(FE_ERR_ARG, "records: class %d out of range", L);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Evaluation launch geometry
 // ---------------------------------------------------------------------------
@@ -213,7 +329,7 @@ struct fe_plan {
   std::vector<double> sexp, scoef;
   std::vector<FeTask> tasks;
   std::vector<int> work_task, work_ij;
-  std::vector<int> grp_block0, grp_code, grp_work0, grp_nwork;
+  std::vector<int> grp_code, grp_work0, grp_nwork;   // (la, lb) groups of work items
   std::vector<long long> class_slot0;   // FE_NCLASS + 1
   std::vector<long long> stage_off;     // FE_NCLASS, in doubles
   std::vector<double> Z, xyz;
@@ -221,7 +337,7 @@ struct fe_plan {
   int nblocks = 0;
   int cap[FE_NCLASS] = {};
   // device blob layout (byte offsets)
-  size_t o_shells, o_sexp, o_scoef, o_tasks, o_wt, o_wij, o_gb, o_gc, o_gw, o_gn, o_cs, o_so;
+  size_t o_shells, o_sexp, o_scoef, o_tasks, o_wt, o_wij, o_cs, o_so;
   size_t plan_bytes = 0;
   size_t table_bytes = 0;
   size_t o_tab64[FE_NCLASS], o_tab32[FE_NCLASS], o_atoms = 0;
@@ -343,7 +459,6 @@ int fe_plan_create(const fe_basis* b, fe_plan** out) {
     }
     const int nw = int(p->work_task.size()) - w0;
     if (nw == 0) continue;
-    p->grp_block0.push_back(block);
     p->grp_code.push_back(code);
     p->grp_work0.push_back(w0);
     p->grp_nwork.push_back(nw);
@@ -359,10 +474,6 @@ int fe_plan_create(const fe_basis* b, fe_plan** out) {
   p->o_tasks = put(sizeof(FeTask) * p->tasks.size());
   p->o_wt = put(sizeof(int) * p->work_task.size());
   p->o_wij = put(sizeof(int) * p->work_ij.size());
-  p->o_gb = put(sizeof(int) * p->grp_block0.size());
-  p->o_gc = put(sizeof(int) * p->grp_code.size());
-  p->o_gw = put(sizeof(int) * p->grp_work0.size());
-  p->o_gn = put(sizeof(int) * p->grp_nwork.size());
   p->o_cs = put(sizeof(long long) * p->class_slot0.size());
   p->o_so = put(sizeof(long long) * p->stage_off.size());
   p->plan_bytes = std::max<size_t>(o, 256);
@@ -419,10 +530,6 @@ int fe_plan_upload(const fe_plan* p, void* d_plan, cudaStream_t st) {
   cp(p->o_tasks, p->tasks.data(), sizeof(FeTask) * p->tasks.size());
   cp(p->o_wt, p->work_task.data(), sizeof(int) * p->work_task.size());
   cp(p->o_wij, p->work_ij.data(), sizeof(int) * p->work_ij.size());
-  cp(p->o_gb, p->grp_block0.data(), sizeof(int) * p->grp_block0.size());
-  cp(p->o_gc, p->grp_code.data(), sizeof(int) * p->grp_code.size());
-  cp(p->o_gw, p->grp_work0.data(), sizeof(int) * p->grp_work0.size());
-  cp(p->o_gn, p->grp_nwork.data(), sizeof(int) * p->grp_nwork.size());
   cp(p->o_cs, p->class_slot0.data(), sizeof(long long) * p->class_slot0.size());
   cp(p->o_so, p->stage_off.data(), sizeof(long long) * p->stage_off.size());
   FE_CUDA(cudaMemcpyAsync(d_plan, h.data(), h.size(), cudaMemcpyHostToDevice, st));
@@ -485,11 +592,6 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
   a.tasks = reinterpret_cast<const FeTask*>(pb + p->o_tasks);
   a.work_task = reinterpret_cast<const int*>(pb + p->o_wt);
   a.work_ij = reinterpret_cast<const int*>(pb + p->o_wij);
-  a.grp_block0 = reinterpret_cast<const int*>(pb + p->o_gb);
-  a.grp_code = reinterpret_cast<const int*>(pb + p->o_gc);
-  a.grp_work0 = reinterpret_cast<const int*>(pb + p->o_gw);
-  a.grp_nwork = reinterpret_cast<const int*>(pb + p->o_gn);
-  a.ngroup = int(p->grp_code.size());
   a.n_func = p->n_func;
   a.dens = d_dens;
   a.pts = d_pts;
@@ -531,8 +633,17 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
   }
   FE_CUDA(cudaMemsetAsync(a.npending, 0, sizeof(int), st));
   if (p->nblocks > 0) {
-    fe_build_kernel<<<p->nblocks, FE_BUILD_THREADS, 0, st>>>(a);
-    FE_CUDA(cudaGetLastError());
+    // the (la, lb) groups side by side, heaviest first
+    const int rc = fork_join(int(p->grp_code.size()), st, [&](int g, cudaStream_t sg) {
+      const FeBuildKernel k = fe_build_kernel_for(p->grp_code[g]);
+      if (!k) return fail(FE_ERR_ARG, "table build: bad group code %d", p->grp_code[g]);
+      const int nw = p->grp_nwork[g];
+      k<<<unsigned((nw + FE_BUILD_THREADS - 1) / FE_BUILD_THREADS), FE_BUILD_THREADS, 0, sg>>>(
+          a, p->grp_work0[g], nw);
+      FE_CUDA(cudaGetLastError());
+      return FE_OK;
+    });
+    if (rc != FE_OK) return rc;
     // pairs whose screen ran past the per-thread budget: one warp each
     fe_screen_pending_kernel<<<sm_count() * 8, 128, 0, st>>>(a);
     FE_CUDA(cudaGetLastError());
@@ -547,14 +658,22 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
     fe_scan_top_kernel<<<1, FE_SCAN_BLOCK, 0, st>>>(bsum, int(nb));
     fe_scan_apply_kernel<<<nb, FE_SCAN_BLOCK, 0, st>>>(a.keep, p->nslot, bsum, pos);
     FE_CUDA(cudaGetLastError());
-    const int thr = 256;
-    fe_scatter_kernel<<<unsigned((p->nslot + thr - 1) / thr), thr, 0, st>>>(
-        a.stage, a.stage_off, a.class_slot0, FE_NCLASS, a.keep, pos, a.swork, p->nslot, tb,
-        float(kTauDefault));
-    FE_CUDA(cudaGetLastError());
+    // per class, side by side: the kept records to their rows, then their FP32
+    // records
+    std::vector<int> cls;
+    for (int L = 0; L < FE_NCLASS; ++L)
+      if (p->class_slot0[L + 1] > p->class_slot0[L]) cls.push_back(L);
+    const int rc = fork_join(int(cls.size()), st, [&](int i, cudaStream_t sg) {
+      const int L = cls[i];
+      const long long c0 = p->class_slot0[L], n = p->class_slot0[L + 1] - c0;
+      const int tile = fe_records_tile_of(L);
+      return launch_records(L, a.stage + p->stage_off[L], a.keep + c0, pos + c0, a.swork + c0,
+                            int(n), tb, unsigned((n + tile - 1) / tile), sg);
+    });
+    if (rc != FE_OK) return rc;
   }
   fe_finalize_kernel<<<1, 1024, 0, st>>>(a.class_slot0, FE_NCLASS, p->nslot, a.keep, pos, bsr,
-                                         tb, float(kTauDefault));
+                                         a.npending, tb, float(kTauDefault));
   FE_CUDA(cudaGetLastError());
   return FE_OK;
 }
@@ -594,9 +713,13 @@ int fe_table_init(void* d_table, const int* count, int n_atoms, const double* Z,
 
 int fe_table_make_f32(void* d_table, cudaStream_t st) {
   if (!d_table) return fail(FE_ERR_ARG, "fe_table_make_f32: null table");
-  fe_make_f32_kernel<<<dim3(std::max(1, 2 * sm_count() / FE_NCLASS), FE_NCLASS), 256, 0, st>>>(
-      static_cast<unsigned char*>(d_table), float(kTauDefault));
-  FE_CUDA(cudaGetLastError());
+  // every class (the counts are in the device header): a grid-stride loop of
+  // two blocks per SM over the class's tiles
+  for (int L = 0; L < FE_NCLASS; ++L) {
+    const int rc = launch_records(L, nullptr, nullptr, nullptr, nullptr, 0,
+                                  static_cast<unsigned char*>(d_table), unsigned(2 * sm_count()), st);
+    if (rc != FE_OK) return rc;
+  }
   return FE_OK;
 }
 
@@ -616,6 +739,7 @@ int fe_table_info_get(const void* d_table, fe_table_info* info, cudaStream_t st)
   info->tol = h.tol;
   info->rule = h.rule;
   info->has_f32 = h.has32;
+  info->n_warp_screen = h.n_warp_screen;
   return FE_OK;
 }
 
@@ -908,33 +1032,6 @@ struct NoallocSlot {
 };
 std::mutex g_noalloc_mu;
 NoallocSlot g_noalloc[FE_NOALLOC_MAX_DEVICES];
-
-using CtxGetCurrentFn = CUresult (*)(CUcontext*);
-using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
-
-// ID of the calling thread's current context (0 when none is current), from
-// the driver's entry points as the runtime hands them out (no link to libcuda).
-unsigned long long current_ctx_id() {
-  static CtxGetCurrentFn get_cur = nullptr;
-  static CtxGetIdFn get_id = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* f = nullptr;
-    cudaDriverEntryPointQueryResult q{};
-    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      get_cur = reinterpret_cast<CtxGetCurrentFn>(f);
-    f = nullptr;
-    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      get_id = reinterpret_cast<CtxGetIdFn>(f);
-  });
-  CUcontext ctx = nullptr;
-  unsigned long long id = 0;
-  if (!get_cur || !get_id || get_cur(&ctx) != CUDA_SUCCESS || !ctx) return 0;
-  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
-  return id;
-}
 
 // The scratch array's device address on the current device.
 int noalloc_scratch(void** out) {

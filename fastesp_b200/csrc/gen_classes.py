@@ -15,7 +15,11 @@ For every angular class L = la + lb (0..8) this emits
   boundaries into chunks of at most MOM_CHUNK terms so the accumulators of a
   chunk stay in registers);
 * the sparse contraction rows M0[k, t] (etab -> G) used by the table builder,
-  with t in the compact order of ``hermite.t_index``;
+  with t in the compact order of ``hermite.t_index``, and for the small
+  classes the same contraction as straight-line code (``fe_m0_rows_L``,
+  ``fe_g_store_L``);
+* ``fe_f32_terms_L``: the coefficient pairs and routing-bound sums of one
+  mixed-precision record, straight-line;
 * the Boys Taylor grid F_n(i h), n = 0..NTAB-1, computed here in 40-digit
   arithmetic (mpmath), and the per-order asymptotic thresholds.
 """
@@ -44,6 +48,7 @@ GRID_TMAX32 = 32.0             # FP32 grid covers 0 <= T < 32 (the FP32 asymptot
 NTAB32 = MMAX + TAYLOR_K32
 VARS = ("x", "y", "z")
 MOM_CHUNK = 48                 # adjoint moment accumulators per thread
+M0_UNROLL_LMAX = 2             # classes whose G contraction is emitted straight-line
 
 
 # --------------------------------------------------------------------------
@@ -236,6 +241,54 @@ def route_constants(L):
         n = 2 * m - deg
         assert 0 <= n <= L and m < 16
         out.append((n, m, math.gamma(m + 0.5) / 2.0 * mf))
+    return out
+
+
+def f32_terms_function(L):
+    """Straight-line FP32-record terms of class L (one thread per record).
+
+    For record position j with routing constants (n, m, c): the coefficient
+    pair o[2j] = o[2j+1] = K G_j s_m v_m and the bound sum b_n += |G_j| c v_m,
+    with v_m = p^-(m+1/2).  Every index is a constant, so s, v and b stay in
+    registers; the operation order is that of a loop over j.
+    """
+    out = [f"// class L={L}: FP32 coefficient pairs and routing-bound sums, record order",
+           f"__device__ __forceinline__ void fe_f32_terms_L{L}(const double* __restrict__ g, double K,",
+           f"    const double (&s)[{L + 1}], const double (&v)[{L + 1}], float* __restrict__ o,",
+           f"    double (&b)[{L + 1}]) {{"]
+    for j, (n, m, c) in enumerate(route_constants(L)):
+        out.append(f"  {{ const double t = g[{j}]; o[{2 * j}] = o[{2 * j + 1}] = float(K * t * s[{m}] * v[{m}]);"
+                   f" b[{n}] += fabs(t) * {c!r} * v[{m}]; }}")
+    out.append("}")
+    return out
+
+
+def m0_functions(L):
+    """Straight-line G contraction of class L for the table builder.
+
+    ``fe_m0_rows_L``: s_k = sum_t M0[k, t] etab[t] for every term k, as fused
+    multiply-adds in the order of the sparse rows; ``fe_g_store_L``: record
+    position j of the term k it holds gets cf (2p)^m_k s_k.  With constant
+    indices the builder keeps etab and s in registers.
+    """
+    keys, rows = H.class_terms(L)
+    tix = H.t_index(L)
+    nt, ntri = len(keys), len(tix)
+    out = [f"// class L={L}: contraction sums s_k = sum_t M0[k, t] etab[t], term order",
+           f"__device__ __forceinline__ void fe_m0_rows_L{L}(const double (&e)[{ntri}], double (&s)[{nt}]) {{"]
+    for k, r in enumerate(rows):
+        (t0, c0), rest = r[0], r[1:]
+        expr = f"{float(c0)!r} * e[{tix[t0]}]"
+        for t, c in rest:
+            expr = f"fma({float(c)!r}, e[{tix[t]}], {expr})"
+        out.append(f"  s[{k}] = {expr};")
+    out.append("}")
+    out.append(f"// class L={L}: G at record position j = cf (2p)^m s_k for the term k stored there")
+    out.append(f"__device__ __forceinline__ void fe_g_store_L{L}(const double (&s)[{nt}],"
+               f" const double (&pw)[{L + 1}], double cf, double* __restrict__ g) {{")
+    for j, k in enumerate(consumption_order(L)):
+        out.append(f"  g[{j}] = cf * pw[{keys[k][3]}] * s[{k}];")
+    out.append("}")
     return out
 
 
@@ -624,6 +677,33 @@ def main() -> int:
     out.append("")
     out.append("static constexpr int fe_class_polyops[FE_NCLASS] = {"
                + ", ".join(map(str, nops)) + "};")
+    out.append("")
+    for L in range(LMAX + 1):
+        out += f32_terms_function(L)
+    out.append("template <int L>")
+    out.append("__device__ __forceinline__ void fe_f32_terms(const double* __restrict__ g, double K,")
+    out.append("    const double (&s)[L + 1], const double (&v)[L + 1], float* __restrict__ o,")
+    out.append("    double (&b)[L + 1]) {")
+    for L in range(LMAX + 1):
+        kw = "if" if L == 0 else "else if"
+        out.append(f"  {kw} constexpr (L == {L}) fe_f32_terms_L{L}(g, K, s, v, o, b);")
+    out.append("}")
+    out.append("")
+    out.append(f"#define FE_M0_UNROLL_LMAX {M0_UNROLL_LMAX}")
+    for L in range(M0_UNROLL_LMAX + 1):
+        out += m0_functions(L)
+    for name, args, call in (
+            ("fe_m0_rows", "const double (&e)[fe_class_ntri[L]], double (&s)[fe_class_nterm[L]]",
+             "(e, s)"),
+            ("fe_g_store", "const double (&s)[fe_class_nterm[L]], const double (&pw)[L + 1], "
+             "double cf, double* __restrict__ g", "(s, pw, cf, g)")):
+        out.append("template <int L>")
+        out.append(f"__device__ __forceinline__ void {name}({args}) {{")
+        out.append("  static_assert(L <= FE_M0_UNROLL_LMAX, \"straight-line contraction not generated\");")
+        for L in range(M0_UNROLL_LMAX + 1):
+            kw = "if" if L == 0 else "else if"
+            out.append(f"  {kw} constexpr (L == {L}) {name}_L{L}{call};")
+        out.append("}")
     out.append("")
     for L in range(LMAX + 1):
         out += grad_function(L)

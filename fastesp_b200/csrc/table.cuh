@@ -54,7 +54,7 @@ struct FeTableHdr {
   int32_t has_src;                   // the source section is filled
   int64_t off_src;                   // byte offset of the source section
   float tau_fast;                    // routing threshold of the FP32 records' far radius
-  int32_t pad_;
+  int32_t n_warp_screen;             // pairs the build's per-thread screen left to the warp screen
 };
 
 static_assert(sizeof(FeTableHdr) <= 512, "header must fit its slot");

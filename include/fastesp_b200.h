@@ -70,6 +70,7 @@ typedef struct fe_table_info {
   double tol;
   int rule;
   int has_f32;
+  int n_warp_screen;       /* pairs of the last device build whose screen took the warp-parallel search */
 } fe_table_info;
 
 /* Version as major*10000 + minor*100 + patch. */
