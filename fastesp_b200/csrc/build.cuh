@@ -616,7 +616,7 @@ FE_DEV long long fe_build_pair(const FeBuildArgs& a, int w) {
   rec[5] = KB;
 #pragma unroll
   for (int k = 6 + NT; k < REC; ++k) rec[k] = 0.0;
-  if (decided == 2) return slot;        // undecided: the block's warps finish it
+  if (decided == 2) return slot;        // undecided: fe_screen_pending_kernel finishes it
   a.keep[slot] = decided;
   return -1;
 }
@@ -632,10 +632,8 @@ FE_DEV long long fe_build_pair(const FeBuildArgs& a, int w) {
 // exceeds the minimum found so far holds no point that lowers it.  The lanes
 // agree on d2min after each superbox (a shuffle reduction), so the decision
 // comes back in every lane.
-FE_DEV bool fe_screen_warp(const FeBuildArgs& a, long long slot, int L, int lane) {
-  const double* rec = a.stage + a.stage_off[L] + (slot - a.class_slot0[L]) * fe_c_rec64[L];
-  const double P[3] = {rec[1], rec[2], rec[3]};
-  const FeScreen sc(a, rec[5], 1.6 * sqrt((L + 2.0) / rec[0]));
+FE_DEV bool fe_screen_warp(const FeBuildArgs& a, const double (&P)[3], const FeScreen& sc,
+                           int lane) {
   double d2min = 1e300;
   bool sure = sc.none;                        // (cannot happen: its thread searched)
   for (int sb0 = 0; sb0 < a.nsbox && !sure; sb0 += 32) {
@@ -684,6 +682,239 @@ FE_DEV bool fe_screen_warp(const FeBuildArgs& a, long long slot, int L, int lane
   return sure || sc.keep_exact(d2min);
 }
 
+// The same for a pending pair, from its staging record.
+FE_DEV bool fe_screen_warp(const FeBuildArgs& a, long long slot, int L, int lane) {
+  const double* rec = a.stage + a.stage_off[L] + (slot - a.class_slot0[L]) * fe_c_rec64[L];
+  const double P[3] = {rec[1], rec[2], rec[3]};
+  const FeScreen sc(a, rec[5], 1.6 * sqrt((L + 2.0) / rec[0]));
+  return fe_screen_warp(a, P, sc, lane);
+}
+
+// Shared-memory doubles per warp of fe_build_pair_warp<LA, LB>: the three E
+// tables, the density block and etab.
+template <int LA, int LB>
+constexpr int fe_warp_pair_smem() {
+  constexpr int L = LA + LB;
+  return 3 * (LA + 1) * (LB + 1) * (L + 1) + (LA + 1) * (LA + 2) / 2 * ((LB + 1) * (LB + 2) / 2) +
+         (L + 1) * (L + 2) * (L + 3) / 6;
+}
+
+// fe_build_pair for the heavy shell-pair groups, one warp per primitive pair:
+// the work a thread would do alone for such a pair (about a hundred density
+// elements, each spread over tens of Hermite entries, and a sparse
+// contraction of over a hundred rows) is split over the lanes, and the point
+// screen is the warp search from the start.  Every number is formed as in
+// fe_build_pair, in the same order, so the records and decisions are the same
+// bit for bit:
+//  * lanes 0-2 compute the x, y, z E tables, kept in shared memory;
+//  * lane l owns the Hermite entries t = l, l + 32, ...: it adds the
+//    contributions of every density element (mu outer, nu inner, as the
+//    thread does) to its entries, in registers;
+//  * lane 0 sums the screening bound over etab in the thread's order;
+//  * lane l owns the contraction rows k = l, l + 32, ...
+// ``sh`` is this warp's fe_warp_pair_smem<LA, LB>() doubles.
+template <int LA, int LB>
+FE_DEV void fe_build_pair_warp(const FeBuildArgs& a, int w, int lane, double* sh) {
+  constexpr int L = LA + LB;
+  constexpr int NA = (LA + 1) * (LA + 2) / 2, NB = (LB + 1) * (LB + 2) / 2;
+  constexpr int NTRI = (L + 1) * (L + 2) * (L + 3) / 6;
+  constexpr int NT = fe_class_nterm[L];
+  constexpr int REC = fe_class_rec64[L];
+  constexpr int NE = (LA + 1) * (LB + 1) * (L + 1);
+  constexpr int RT = (NTRI + 31) / 32, RK = (NT + 31) / 32;
+  double* sE = sh;                     // [3][LA+1][LB+1][L+1]
+  double* sW = sh + 3 * NE;            // [NA][NB]
+  double* sT = sW + NA * NB;           // etab[NTRI]
+  const FeTask tk = a.tasks[a.work_task[w]];
+  const int ij = a.work_ij[w];
+  const int ii = ij >> 16, jj = ij & 0xffff;
+  const FeShell& A = a.shells[tk.si];
+  const FeShell& B = a.shells[tk.sj];
+  const long long slot = a.class_slot0[L] + tk.slot0 + ii * B.nprim + jj;
+  if (lane == 0) {
+    a.keep[slot] = 0;
+    a.srule[slot] = 0.0;
+    a.swork[slot] = w;
+  }
+  // density block (both orderings for si != sj)
+  double wmax = 0.0;
+  for (int c = lane; c < NA * NB; c += 32) {
+    const int mu = c / NB, nu = c - mu * NB;
+    double d = a.dens[size_t(A.fn0 + mu) * a.n_func + (B.fn0 + nu)];
+    if (tk.si != tk.sj) d += a.dens[size_t(B.fn0 + nu) * a.n_func + (A.fn0 + mu)];
+    sW[c] = d;
+    wmax = fmax(wmax, fabs(d));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) wmax = fmax(wmax, __shfl_xor_sync(0xffffffffu, wmax, o));
+  if (!(wmax >= 1e-15)) return;
+
+  const double al = a.sexp[A.prim0 + ii], be = a.sexp[B.prim0 + jj];
+  const double cc = a.scoef[A.prim0 + ii] * a.scoef[B.prim0 + jj];
+  const double p = al + be;
+  double ab2 = 0.0, P[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double d = A.c[k] - B.c[k];
+    ab2 += d * d;
+  }
+  const double K = exp(-(al * be) / p * ab2);
+  if (!(K >= 1e-30)) return;
+  if (a.rule == 1 && cc == 0.0) return;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) P[k] = (al * A.c[k] + be * B.c[k]) / p;
+  const double ip = 1.0 / (2.0 * p);
+  if (lane < 3) {
+    double e[LA + 1][LB + 1][L + 1];
+    fe_hermite_1d<LA, LB>(ip, P[lane] - A.c[lane], P[lane] - B.c[lane], e);
+    double* dst = sE + lane * NE;
+#pragma unroll
+    for (int i = 0; i <= LA; ++i)
+#pragma unroll
+      for (int j = 0; j <= LB; ++j)
+#pragma unroll
+        for (int t = 0; t <= L; ++t) dst[(i * (LB + 1) + j) * (L + 1) + t] = e[i][j][t];
+  }
+  __syncwarp();
+
+  // this lane's Hermite entries: t = lane + 32 r in the compact x-major order
+  int tx[RT], ty[RT], tz[RT];
+  double acc[RT];
+#pragma unroll
+  for (int r = 0; r < RT; ++r) {
+    acc[r] = 0.0;
+    tx[r] = ty[r] = tz[r] = L + 1;               // beyond every a + b: never added to
+    int t = lane + 32 * r, n = 0;
+    for (int x = 0; x <= L; ++x)
+      for (int y = 0; y <= L - x; ++y)
+        for (int z = 0; z <= L - x - y; ++z, ++n)
+          if (n == t) {
+            tx[r] = x;
+            ty[r] = y;
+            tz[r] = z;
+          }
+  }
+  const double* EX = sE;
+  const double* EY = sE + NE;
+  const double* EZ = sE + 2 * NE;
+#pragma unroll 1
+  for (int mu = 0; mu < NA; ++mu) {
+    const int ax = fe_cart[LA][mu][0], ay = fe_cart[LA][mu][1], az = fe_cart[LA][mu][2];
+#pragma unroll 1
+    for (int nu = 0; nu < NB; ++nu) {
+      const double wt = sW[mu * NB + nu] * cc;
+      const int bx = fe_cart[LB][nu][0], by = fe_cart[LB][nu][1], bz = fe_cart[LB][nu][2];
+#pragma unroll
+      for (int r = 0; r < RT; ++r)
+        if (tx[r] <= ax + bx && ty[r] <= ay + by && tz[r] <= az + bz) {
+          const double vx = wt * EX[(ax * (LB + 1) + bx) * (L + 1) + tx[r]];
+          const double vxy = vx * EY[(ay * (LB + 1) + by) * (L + 1) + ty[r]];
+          acc[r] += vxy * EZ[(az * (LB + 1) + bz) * (L + 1) + tz[r]];
+        }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < RT; ++r)
+    if (lane + 32 * r < NTRI) sT[lane + 32 * r] = acc[r];
+  __syncwarp();
+  // sum rule: int rho_pair = K (pi/p)^1.5 etab[0]   (build_pairs.cpp:294-296)
+  if (lane == 0) a.srule[slot] = K * pow(3.14159265358979323846 / p, 1.5) * sT[0];
+
+  // this lane's contraction sums: rows k = lane + 32 r
+  const double tp = 2.0 * p;
+  const short* rp = fe_m0_ptr<L>();
+  const short* rc = fe_m0_col<L>();
+  const float* rv = fe_m0_val<L>();
+  const signed char* rm = fe_m0_m<L>();
+  double gsum[RK];
+  bool anyg = false;
+#pragma unroll
+  for (int r = 0; r < RK; ++r) {
+    const int k = lane + 32 * r;
+    double sk = 0.0;
+    if (k < NT)
+      for (int q = rp[k]; q < rp[k + 1]; ++q) sk += double(rv[q]) * sT[rc[q]];
+    gsum[r] = sk;
+    anyg |= sk != 0.0;
+  }
+  // the C++ builder drops pairs whose G are all zero (build_pairs.cpp:309)
+  if (a.rule == 1 && !__any_sync(0xffffffffu, anyg)) return;
+
+  // screening bound (esp.py:251-254), summed by lane 0 in the thread's order
+  double KB = 0.0;
+  if (lane == 0) {
+    const double sq = sqrt(tp);
+    double sqp[L + 1];
+    sqp[0] = 1.0;
+#pragma unroll
+    for (int m = 1; m <= L; ++m) sqp[m] = sqp[m - 1] * sq;
+    double bsum = 0.0;
+#pragma unroll
+    for (int x = 0; x <= L; ++x)
+#pragma unroll
+      for (int y = 0; y <= L - x; ++y)
+#pragma unroll
+        for (int z = 0; z <= L - x - y; ++z)
+          bsum += fabs(sT[fe_tri<L>(x, y, z)]) * (fe_screen_mom[x] * fe_screen_mom[y]
+                   * fe_screen_mom[z]) * sqp[x + y + z];
+    const double bound = pow(tp, -1.5) * bsum;
+    KB = __dmul_rn(K, bound);
+  }
+  KB = __shfl_sync(0xffffffffu, KB, 0);
+  const double reff = 1.6 * sqrt((L + 2.0) / p);
+  bool keep;
+  if (a.npts == 0 || a.tol <= 0.0) {
+    keep = true;                                 // no points, or tol 0: every pair is kept
+  } else {
+    const FeScreen sc(a, KB, reff);
+    keep = !sc.none && fe_screen_warp(a, P, sc, lane);
+  }
+  if (!keep) return;
+
+  // G_k = (2 pi / p) (2p)^m_k sum_t M0[k,t] etab[t], at record position fe_gpos_L[k]
+  const double cf = 2.0 * 3.14159265358979323846 / p;
+  double pw[L + 1];
+  pw[0] = 1.0;
+#pragma unroll
+  for (int m = 1; m <= L; ++m) pw[m] = pw[m - 1] * tp;
+  double* rec = a.stage + a.stage_off[L] + (slot - a.class_slot0[L]) * REC;
+  const short* gpos = fe_gpos<L>();
+#pragma unroll
+  for (int r = 0; r < RK; ++r) {
+    const int k = lane + 32 * r;
+    if (k < NT) rec[6 + gpos[k]] = cf * pw[rm[k]] * gsum[r];
+  }
+  if (lane == 0) {
+    rec[0] = p;
+    rec[1] = P[0];
+    rec[2] = P[1];
+    rec[3] = P[2];
+    rec[4] = K;
+    rec[5] = KB;
+  }
+  for (int k = 6 + NT + lane; k < REC; k += 32) rec[k] = 0.0;
+  if (lane == 0) a.keep[slot] = 1;
+}
+
+// Groups whose pairs take one warp each: those with at least this many
+// density elements per shell pair (p-f and up; d-d).
+#ifndef FE_WARP_PAIR_MIN
+#define FE_WARP_PAIR_MIN 30
+#endif
+__host__ __device__ constexpr bool fe_warp_pair_group(int la, int lb) {
+  return (la + 1) * (la + 2) / 2 * ((lb + 1) * (lb + 2) / 2) >= FE_WARP_PAIR_MIN;
+}
+
+template <int LA, int LB>
+__global__ void __launch_bounds__(128) fe_build_warp_kernel(const FeBuildArgs a, int work0,
+                                                            int nwork) {
+  constexpr int SH = fe_warp_pair_smem<LA, LB>();
+  __shared__ double sh[4 * SH];
+  const int wid = int(threadIdx.x >> 5);
+  const int w = int(blockIdx.x) * 4 + wid;
+  if (w < nwork) fe_build_pair_warp<LA, LB>(a, work0 + w, int(threadIdx.x & 31), sh + wid * SH);
+}
+
 #define FE_BUILD_THREADS 128
 
 // One launch per (la, lb) group of work items (all primitive pairs of the
@@ -727,9 +958,16 @@ __global__ void __launch_bounds__(128) fe_screen_pending_kernel(const FeBuildArg
 
 using FeBuildKernel = void (*)(const FeBuildArgs, int, int);
 
-// The group kernel of code la * 5 + lb.
+// The kernel of group la * 5 + lb: fe_build_warp_kernel (one warp per pair,
+// FE_BUILD_THREADS / 32 pairs per block) for the heavy groups,
+// fe_build_kernel (one thread per pair) for the rest.
+template <int LA, int LB>
+constexpr FeBuildKernel fe_group_kernel() {
+  if constexpr (fe_warp_pair_group(LA, LB)) return fe_build_warp_kernel<LA, LB>;
+  else return fe_build_kernel<LA, LB>;
+}
 inline FeBuildKernel fe_build_kernel_for(int code) {
-#define FE_K(la, lb) fe_build_kernel<la, lb>,
+#define FE_K(la, lb) fe_group_kernel<la, lb>(),
   static const FeBuildKernel k[25] = {
     FE_K(0, 0) FE_K(0, 1) FE_K(0, 2) FE_K(0, 3) FE_K(0, 4)
     FE_K(1, 0) FE_K(1, 1) FE_K(1, 2) FE_K(1, 3) FE_K(1, 4)
@@ -738,6 +976,10 @@ inline FeBuildKernel fe_build_kernel_for(int code) {
     FE_K(4, 0) FE_K(4, 1) FE_K(4, 2) FE_K(4, 3) FE_K(4, 4)};
 #undef FE_K
   return code >= 0 && code < 25 ? k[code] : nullptr;
+}
+// Pairs per block of group la * 5 + lb's kernel.
+inline int fe_build_pairs_per_block(int code) {
+  return fe_warp_pair_group(code / 5, code % 5) ? FE_BUILD_THREADS / 32 : FE_BUILD_THREADS;
 }
 
 // log2(x) for finite x > 0 and 2^y to about 1e-6 relative (float MUFU on the

@@ -637,9 +637,8 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
     const int rc = fork_join(int(p->grp_code.size()), st, [&](int g, cudaStream_t sg) {
       const FeBuildKernel k = fe_build_kernel_for(p->grp_code[g]);
       if (!k) return fail(FE_ERR_ARG, "table build: bad group code %d", p->grp_code[g]);
-      const int nw = p->grp_nwork[g];
-      k<<<unsigned((nw + FE_BUILD_THREADS - 1) / FE_BUILD_THREADS), FE_BUILD_THREADS, 0, sg>>>(
-          a, p->grp_work0[g], nw);
+      const int nw = p->grp_nwork[g], per = fe_build_pairs_per_block(p->grp_code[g]);
+      k<<<unsigned((nw + per - 1) / per), FE_BUILD_THREADS, 0, sg>>>(a, p->grp_work0[g], nw);
       FE_CUDA(cudaGetLastError());
       return FE_OK;
     });
