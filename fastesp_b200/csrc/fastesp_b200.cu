@@ -138,6 +138,37 @@ int side_streams(SideStreams** out) {
 // side streams used; the side streams start after the work already on ``st``
 // and every later launch on ``st`` waits for them.  The side streams are
 // joined even when a launch fails.
+// Two sets side by side: set A (na items) on the caller's stream and the first
+// side streams, set B (nb items) on the others; once set A is done,
+// after_a(st) runs on the caller's stream while set B may still run; later
+// launches on ``st`` wait for both sets.
+template <typename FA, typename FM, typename FB>
+int fork_join2(int na, int nb, cudaStream_t st, FA&& launch_a, FM&& after_a, FB&& launch_b) {
+  std::lock_guard<std::mutex> lock(g_side_mu);
+  SideStreams* ss = nullptr;
+  int rc = side_streams(&ss);
+  if (rc != FE_OK) return rc;
+  const int kb = nb > 0 ? std::min(nb, FE_SIDE_STREAMS / 2) : 0;
+  const int ka = std::min(std::max(na - 1, 0), FE_SIDE_STREAMS - kb);
+  if (ka + kb > 0) FE_CUDA(cudaEventRecord(ss->fork, st));
+  for (int i = 0; i < ka + kb; ++i) FE_CUDA(cudaStreamWaitEvent(ss->s[i], ss->fork, 0));
+  for (int i = 0; i < na && rc == FE_OK; ++i) {
+    const int q = i % (ka + 1);
+    rc = launch_a(i, q == 0 ? st : ss->s[q - 1]);
+  }
+  for (int i = 0; i < nb && rc == FE_OK; ++i) rc = launch_b(i, ss->s[ka + i % kb]);
+  for (int i = 0; i < ka; ++i) {
+    FE_CUDA(cudaEventRecord(ss->join[i], ss->s[i]));
+    FE_CUDA(cudaStreamWaitEvent(st, ss->join[i], 0));
+  }
+  if (rc == FE_OK) rc = after_a(st);
+  for (int i = ka; i < ka + kb; ++i) {
+    FE_CUDA(cudaEventRecord(ss->join[i], ss->s[i]));
+    FE_CUDA(cudaStreamWaitEvent(st, ss->join[i], 0));
+  }
+  return rc;
+}
+
 template <typename F>
 int fork_join(int n, cudaStream_t st, F&& launch) {
   if (n <= 0) return FE_OK;
@@ -633,19 +664,29 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
   }
   FE_CUDA(cudaMemsetAsync(a.npending, 0, sizeof(int), st));
   if (p->nblocks > 0) {
-    // the (la, lb) groups side by side, heaviest first
-    const int rc = fork_join(int(p->grp_code.size()), st, [&](int g, cudaStream_t sg) {
+    // the (la, lb) groups side by side, heaviest first: the thread-per-pair
+    // groups, then the pairs their threads left undecided (one warp each),
+    // while the warp-per-pair groups (which leave none) run beside them
+    std::vector<int> tg, wg;
+    for (int g = 0; g < int(p->grp_code.size()); ++g)
+      (fe_build_pairs_per_block(p->grp_code[g]) == FE_BUILD_THREADS ? tg : wg).push_back(g);
+    auto group = [&](int g, cudaStream_t sg) {
       const FeBuildKernel k = fe_build_kernel_for(p->grp_code[g]);
       if (!k) return fail(FE_ERR_ARG, "table build: bad group code %d", p->grp_code[g]);
       const int nw = p->grp_nwork[g], per = fe_build_pairs_per_block(p->grp_code[g]);
       k<<<unsigned((nw + per - 1) / per), FE_BUILD_THREADS, 0, sg>>>(a, p->grp_work0[g], nw);
       FE_CUDA(cudaGetLastError());
       return FE_OK;
-    });
+    };
+    const int rc = fork_join2(
+        int(tg.size()), int(wg.size()), st, [&](int i, cudaStream_t sg) { return group(tg[i], sg); },
+        [&](cudaStream_t s0) {
+          fe_screen_pending_kernel<<<sm_count() * 8, 128, 0, s0>>>(a);
+          FE_CUDA(cudaGetLastError());
+          return FE_OK;
+        },
+        [&](int i, cudaStream_t sg) { return group(wg[i], sg); });
     if (rc != FE_OK) return rc;
-    // pairs whose screen ran past the per-thread budget: one warp each
-    fe_screen_pending_kernel<<<sm_count() * 8, 128, 0, st>>>(a);
-    FE_CUDA(cudaGetLastError());
   }
   int* pos = reinterpret_cast<int*>(wb + p->ws_pos);
   double* bsr = reinterpret_cast<double*>(wb + p->ws_bsr);
