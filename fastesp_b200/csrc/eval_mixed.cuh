@@ -369,15 +369,19 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_f32_kernel(const FeMix
 // (fe_class_rows, class-major so that concurrently running blocks execute the
 // same class's code).  Each warp walks its own mask row, 32 words at a time
 // (one word per lane, the non-empty ones found by a ballot), and evaluates
-// every pair whose bit is set for its points, reading the pair's FP64 record
-// with warp-uniform loads (L1/L2: the warps of a block that route the same pair
-// read it at about the same time).  No block barrier: a warp with nothing
+// every pair whose bit is set for its points.  The pair's FP64 record comes
+// into the warp's own shared-memory buffer by cp.async, the next routed pair's
+// while the warp evaluates the current one (two buffers), so the coefficient
+// reads are shared-memory broadcasts rather than L1 round trips on the
+// critical path.  No block barrier: a warp with nothing
 // routed finishes early.  Every warp accumulates its pairs in pair order and
 // every grid row writes its own partial sums, so the result is deterministic.
 template <int MINB, int LLO, int LHI>
 __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_fix64_kernel(const FeMixedArgs a) {
   constexpr int NP = FE_MX_NP, NT = FE_MX_NT, NW = FE_MX_NT / 32;
+  constexpr int RMAX = fe_class_rec64[LHI];          // largest record of the range
   __shared__ FeBlockWork w;
+  __shared__ __align__(16) double fix_rec[NW][2][RMAX];
   const FeTableHdr* hdr = reinterpret_cast<const FeTableHdr*>(a.table);
   const int tid = threadIdx.x, lane = tid & 31, wi = tid >> 5;
   double cx[NP], cy[NP], cz[NP], a64[NP];
@@ -410,24 +414,61 @@ __global__ void __launch_bounds__(FE_MX_NT, MINB) fe_eval_fix64_kernel(const FeM
     const int S64 = fe_c_rec64[L];
     const double* base = reinterpret_cast<const double*>(a.table + hdr->off64[L]);
     const unsigned* mrow = a.mask + (warp0 + wi) * w.wtotal + w.woff[L];
-    for (int c0 = w0; c0 < w1; c0 += 32) {
-      const unsigned wv = c0 + lane < w1 ? mrow[c0 + lane] : 0u;
-      unsigned nz = __ballot_sync(0xffffffffu, wv != 0u);
-      while (nz) {                                    // warp-uniform
-        const int k = __ffs(nz) - 1;
-        nz &= nz - 1;
-        unsigned mine = __shfl_sync(0xffffffffu, wv, k);
-        const size_t pair0 = size_t(c0 + k) * 32;
-        while (mine) {
+    // the warp's routed pairs in order: mask words 32 at a time (one per
+    // lane), then the set bits of each non-zero word (warp-uniform state)
+    int c0 = w0 - 32;
+    unsigned wv = 0u, nz = 0u, mine = 0u;
+    long long pair0 = 0;
+    auto next = [&]() -> long long {
+      for (;;) {
+        if (mine) {
           const int bit = __ffs(mine) - 1;
           mine &= mine - 1;
-          ++n64;
-          const double* rec = base + (pair0 + bit) * S64;
-#define FE_CALLP(l) fe_pair_fix64<l, NP>(rec, cx, cy, cz, a64)
-          FE_MX_SWITCH(FE_CALLP)
-#undef FE_CALLP
+          return pair0 + bit;
         }
+        if (nz) {
+          const int k = __ffs(nz) - 1;
+          nz &= nz - 1;
+          mine = __shfl_sync(0xffffffffu, wv, k);
+          pair0 = (long long)(c0 + k) * 32;
+          continue;
+        }
+        c0 += 32;
+        if (c0 >= w1) return -1;
+        wv = c0 + lane < w1 ? mrow[c0 + lane] : 0u;
+        nz = __ballot_sync(0xffffffffu, wv != 0u);
       }
+    };
+    // each routed pair's FP64 record is copied to this warp's shared buffer
+    // (16-byte cp.async by the lanes) while the warp evaluates the previous one
+    auto fetch = [&](long long pr, int b) {
+      const double* src = base + pr * S64;
+      double* dst = fix_rec[wi][b];
+      for (int c = lane; c < S64 / 2; c += 32)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst + 2 * c)),
+                     "l"(src + 2 * c) : "memory");
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    long long cur = next();
+    int b = 0;
+    if (cur >= 0) fetch(cur, 0);
+    while (cur >= 0) {                                // warp-uniform
+      const long long nxt = next();
+      if (nxt >= 0) {
+        fetch(nxt, b ^ 1);
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+      } else {
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+      }
+      __syncwarp();
+      ++n64;
+      const double* rec = fix_rec[wi][b];
+#define FE_CALLP(l) fe_pair_fix64<l, NP>(rec, cx, cy, cz, a64)
+      FE_MX_SWITCH(FE_CALLP)
+#undef FE_CALLP
+      __syncwarp();                                   // before the buffer is refilled
+      cur = nxt;
+      b ^= 1;
     }
   }
   if (a.n64 && lane == 0) atomicAdd(a.n64, (unsigned long long)n64);

@@ -133,11 +133,6 @@ int side_streams(SideStreams** out) {
   return FE_OK;
 }
 
-// Run launch(i, stream) for i = 0..n-1 side by side: item i goes to the
-// caller's stream (i % (k + 1) == 0) or side stream i % (k + 1) - 1, k the
-// side streams used; the side streams start after the work already on ``st``
-// and every later launch on ``st`` waits for them.  The side streams are
-// joined even when a launch fails.
 // Two sets side by side: set A (na items) on the caller's stream and the first
 // side streams, set B (nb items) on the others; once set A is done,
 // after_a(st) runs on the caller's stream while set B may still run; later
@@ -169,6 +164,11 @@ int fork_join2(int na, int nb, cudaStream_t st, FA&& launch_a, FM&& after_a, FB&
   return rc;
 }
 
+// Run launch(i, stream) for i = 0..n-1 side by side: item i goes to the
+// caller's stream (i % (k + 1) == 0) or side stream i % (k + 1) - 1, k the
+// side streams used; the side streams start after the work already on ``st``
+// and every later launch on ``st`` waits for them.  The side streams are
+// joined even when a launch fails.
 template <typename F>
 int fork_join(int n, cudaStream_t st, F&& launch) {
   if (n <= 0) return FE_OK;
