@@ -75,6 +75,7 @@ _SIGS = {
     "fe_table_make_f32": (C.c_int, [_P, _P]),
     "fe_table_info_get": (C.c_int, [_P, C.POINTER(FeTableInfo), _P]),
     "fe_eval_ws_bytes": (C.c_size_t, [C.c_int]),
+    "fe_point_order_bytes": (C.c_size_t, [C.c_int]),
     "fe_eval_ws_bytes_mixed": (C.c_size_t, [C.c_int, C.POINTER(C.c_int)]),
     "fe_esp_fp64": (C.c_int, [_P, _P, C.c_int, _P, _P, C.c_size_t, _P]),
     "fe_electron_fp64": (C.c_int, [_P, _P, C.c_int, _P, _P, C.c_size_t, _P]),
@@ -164,9 +165,10 @@ def stream_ptr(stream=None) -> int:
 
 
 def ws_bytes(n_pts: int, precision: str = "fp64", caps=None) -> int:
-    """Evaluation workspace bytes (``caps``: per-class pair bounds, mixed only)."""
+    """Evaluation workspace bytes (``caps``: per-class pair bounds, mixed only),
+    with room for the evaluators' spatial point order."""
     L = lib()
     if precision == "fp64":
-        return int(L.fe_eval_ws_bytes(int(n_pts)))
+        return int(L.fe_eval_ws_bytes(int(n_pts))) + int(L.fe_point_order_bytes(int(n_pts)))
     cap = (C.c_int * NCLASS)(*[int(c) for c in caps])
     return int(L.fe_eval_ws_bytes_mixed(int(n_pts), cap))

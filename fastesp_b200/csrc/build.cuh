@@ -268,20 +268,26 @@ __global__ void __launch_bounds__(256) fe_points_bbox_kernel(const double* __res
   }
 }
 
+// Morton code of the cell holding point q in a grid of 2^BITS cells per axis
+// over the bounding box bb = [lo, hi].
+template <int BITS>
 FE_DEV int fe_morton_cell(const double* __restrict__ q, const double* __restrict__ bb) {
+  constexpr int N = 1 << BITS;
   int code = 0;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const double ext = bb[3 + k] - bb[k];
-    const double cs = ext > 0.0 ? ext * (1.0 / 16.0) * (1.0 + 1e-9) : 1.0;
+    const double cs = ext > 0.0 ? ext * (1.0 / N) * (1.0 + 1e-9) : 1.0;
     // fmax/fmin first: a NaN coordinate goes to cell 0
-    const int c = int(fmin(fmax((q[k] - bb[k]) / cs, 0.0), 15.0));
+    const int c = int(fmin(fmax((q[k] - bb[k]) / cs, 0.0), double(N - 1)));
 #pragma unroll
-    for (int b = 0; b < 4; ++b) code |= ((c >> b) & 1) << (3 * b + k);
+    for (int b = 0; b < BITS; ++b) code |= ((c >> b) & 1) << (3 * b + k);
   }
   return code;
 }
 
+// cell[q] and the per-cell counts (2^(3 BITS) cells, counts zeroed by the caller).
+template <int BITS>
 __global__ void fe_points_count_kernel(const double* __restrict__ pts, int npts,
                                        const double* __restrict__ bbp, int* __restrict__ cell,
                                        int* __restrict__ count) {
@@ -295,7 +301,7 @@ __global__ void fe_points_count_kernel(const double* __restrict__ pts, int npts,
   __syncthreads();
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= npts) return;
-  const int c = fe_morton_cell(pts + 3 * q, bb);
+  const int c = fe_morton_cell<BITS>(pts + 3 * q, bb);
   cell[q] = c;
   atomicAdd(count + c, 1);
 }
@@ -1297,3 +1303,52 @@ __global__ void __launch_bounds__(FE_SCAN_BLOCK) fe_scan_apply_kernel(
   if (i < n) pos[i] = bsum[blockIdx.x] + buf[threadIdx.x] - v;
 }
 
+
+// ---------------------------------------------------------------------------
+// Spatial order of the evaluation points
+// ---------------------------------------------------------------------------
+// The evaluators decide per warp of points (the mixed path's FP64 routing and
+// far-pair test) and branch per warp (the Boys regimes), so a warp whose points
+// lie close together does less work than one spread over the molecule.  With
+// room in the workspace, the points are evaluated in the order of the Morton
+// code of a 32^3 grid of cells over their bounding box, in the caller's order
+// within a cell (a stable counting sort: the order, and so every result, is
+// the same from run to run), and every result goes back to its caller's row.
+#define FE_ORDER_BITS 5
+#define FE_ORDER_CELLS (1 << (3 * FE_ORDER_BITS))
+
+// idx: the points grouped by cell, in any order within a cell (``cursor``
+// starts as the cells' first positions and ends as their ends).
+__global__ void fe_order_place_kernel(const int* __restrict__ cell, int npts,
+                                      int* __restrict__ cursor, int* __restrict__ idx) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= npts) return;
+  const int at = atomicAdd(cursor + cell[q], 1);
+  if (at < 0 || at >= npts) {
+    fe_flag(FE_ST_OVERFLOW);
+    return;
+  }
+  idx[at] = q;
+}
+
+// Point q's final position: its cell's first position plus the number of the
+// cell's points with a smaller caller index.  sorted[pos] = pts[q], perm[pos] = q.
+__global__ void fe_order_rank_kernel(const double* __restrict__ pts, int npts,
+                                     const int* __restrict__ cell, const int* __restrict__ start,
+                                     const int* __restrict__ end, const int* __restrict__ idx,
+                                     double* __restrict__ sorted, int* __restrict__ perm) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= npts) return;
+  const int c = cell[q];
+  const int s = start[c], e = min(end[c], npts);
+  int r = 0;
+  for (int i = s; i < e; ++i) r += idx[i] < q;
+  const int pos = s + r;
+  if (pos < 0 || pos >= npts) {
+    fe_flag(FE_ST_OVERFLOW);
+    return;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) sorted[3 * pos + k] = pts[3 * q + k];
+  perm[pos] = q;
+}

@@ -284,22 +284,25 @@ __global__ void __launch_bounds__(NT, MINB) fe_eval_f64_kernel(const FeEvalArgs 
   }
 }
 
-// out[i] = nuclear(i) - sum_s partial[s][i] (mode 0) or the sum alone (mode 1);
-// splits are added in order.
+// out[perm[i]] = nuclear(i) - sum_s partial[s][i] (mode 0) or the sum alone
+// (mode 1); splits are added in order.  ``perm`` (the caller's row of
+// evaluated point i) may be null: the identity.
 __global__ void fe_reduce_kernel(const unsigned char* table, const double* __restrict__ pts,
                                  int npts, const double* __restrict__ partial, int nsplit,
-                                 int ld, double* __restrict__ out, int mode) {
+                                 int ld, double* __restrict__ out, int mode,
+                                 const int* __restrict__ perm) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= npts) return;
   const FeTableHdr* hdr = reinterpret_cast<const FeTableHdr*>(table);
+  const int o = perm ? perm[i] : i;
   double e = 0.0;
   for (int s = 0; s < nsplit; ++s) e += partial[size_t(s) * ld + i];
   if (mode == 1) {
-    out[i] = e;
+    out[o] = e;
     return;
   }
   const double* Z = reinterpret_cast<const double*>(table + hdr->off_atoms);
-  out[i] = fe_nuclear(Z, Z + hdr->n_atoms, hdr->n_atoms, pts[3 * i], pts[3 * i + 1],
+  out[o] = fe_nuclear(Z, Z + hdr->n_atoms, hdr->n_atoms, pts[3 * i], pts[3 * i + 1],
                       pts[3 * i + 2]) - e;
 }
 

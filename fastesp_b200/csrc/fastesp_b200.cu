@@ -652,7 +652,7 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
     double* bb = reinterpret_cast<double*>(wb + pw.bb);
     FE_CUDA(cudaMemsetAsync(count, 0, (FE_SORT_CELLS + 1) * sizeof(int), st));
     fe_points_bbox_kernel<<<FE_BBOX_BLOCKS, 256, 0, st>>>(d_pts, n_pts, bb);
-    fe_points_count_kernel<<<(n_pts + 255) / 256, 256, 0, st>>>(d_pts, n_pts, bb, cell, count);
+    fe_points_count_kernel<4><<<(n_pts + 255) / 256, 256, 0, st>>>(d_pts, n_pts, bb, cell, count);
     fe_scan_top_kernel<<<1, FE_SCAN_BLOCK, 0, st>>>(count, FE_SORT_CELLS);
     fe_points_place_kernel<<<(n_pts + 255) / 256, 256, 0, st>>>(d_pts, n_pts, cell, count, sorted);
     FE_CUDA(cudaGetLastError());
@@ -783,6 +783,56 @@ int fe_table_info_get(const void* d_table, fe_table_info* info, cudaStream_t st)
   return FE_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Workspace section of the spatial point order (after the partial rows):
+// the points in evaluation order, each one's caller row, the cells, the
+// points grouped by cell, the per-cell starts and ends, the bounding boxes.
+struct OrderWs {
+  size_t pts, perm, cell, idx, start, end, bb, bytes;
+};
+OrderWs order_ws(int n) {
+  OrderWs w{};
+  size_t o = 0;
+  auto put = [&](size_t b) { const size_t at = o; o = align256(o + b); return at; };
+  w.pts = put(size_t(n) * 3 * sizeof(double));
+  w.perm = put(size_t(n) * sizeof(int));
+  w.cell = put(size_t(n) * sizeof(int));
+  w.idx = put(size_t(n) * sizeof(int));
+  w.start = put((FE_ORDER_CELLS + 1) * sizeof(int));
+  w.end = put((FE_ORDER_CELLS + 1) * sizeof(int));
+  w.bb = put(6 * FE_BBOX_BLOCKS * sizeof(double));
+  w.bytes = o;
+  return w;
+}
+
+// The points of d_pts in evaluation order into the section at ``ob``.
+int order_points(const double* d_pts, int n, unsigned char* ob, const OrderWs& w, cudaStream_t st) {
+  int* cell = reinterpret_cast<int*>(ob + w.cell);
+  int* start = reinterpret_cast<int*>(ob + w.start);
+  int* end = reinterpret_cast<int*>(ob + w.end);
+  double* bb = reinterpret_cast<double*>(ob + w.bb);
+  FE_CUDA(cudaMemsetAsync(start, 0, (FE_ORDER_CELLS + 1) * sizeof(int), st));
+  fe_points_bbox_kernel<<<FE_BBOX_BLOCKS, 256, 0, st>>>(d_pts, n, bb);
+  fe_points_count_kernel<FE_ORDER_BITS><<<(n + 255) / 256, 256, 0, st>>>(d_pts, n, bb, cell, start);
+  fe_scan_top_kernel<<<1, FE_SCAN_BLOCK, 0, st>>>(start, FE_ORDER_CELLS);
+  FE_CUDA(cudaGetLastError());
+  FE_CUDA(cudaMemcpyAsync(end, start, FE_ORDER_CELLS * sizeof(int), cudaMemcpyDeviceToDevice, st));
+  fe_order_place_kernel<<<(n + 255) / 256, 256, 0, st>>>(cell, n, end,
+                                                         reinterpret_cast<int*>(ob + w.idx));
+  fe_order_rank_kernel<<<(n + 255) / 256, 256, 0, st>>>(
+      d_pts, n, cell, start, end, reinterpret_cast<const int*>(ob + w.idx),
+      reinterpret_cast<double*>(ob + w.pts), reinterpret_cast<int*>(ob + w.perm));
+  FE_CUDA(cudaGetLastError());
+  return FE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 size_t fe_eval_ws_bytes(int n_pts) {
   if (n_pts <= 0) return 256;
   const EvalGeom g = eval_geom(n_pts, 0);
@@ -795,8 +845,11 @@ size_t fe_eval_ws_bytes_mixed(int n_pts, const int* cap) {
   long long words = 0;
   for (int L = 0; L < FE_NCLASS; ++L) words += cap ? (std::max(cap[L], 0) + 31) / 32 : 0;
   const long long warps = (long long)g.nblk_x * (FE_MX_NT / 32);
-  return align256(g.ws_rows() * g.ld * sizeof(double)) + align256(size_t(warps * words) * 4);
+  return align256(g.ws_rows() * g.ld * sizeof(double)) + order_ws(n_pts).bytes +
+         align256(size_t(warps * words) * 4);
 }
+
+size_t fe_point_order_bytes(int n_pts) { return n_pts > 0 ? order_ws(n_pts).bytes : 0; }
 
 }  // extern "C"
 
@@ -813,6 +866,19 @@ int eval_launch(const char* who, const void* d_table, const double* d_pts, int n
   const size_t rows_bytes = align256(g.ws_rows() * g.ld * sizeof(double));
   if (!d_ws || ws_bytes < rows_bytes)
     return fail(FE_ERR_SIZE, "%s: workspace too small (need at least %zu bytes)", who, rows_bytes);
+  // the points in spatial order when the workspace has room for it (after the
+  // rows); the mixed path's routing mask takes what follows
+  size_t used = rows_bytes;
+  const int* perm = nullptr;
+  const OrderWs ow = order_ws(n_pts);
+  if (ws_bytes >= rows_bytes + ow.bytes + (prec ? 4 : 0)) {
+    unsigned char* ob = static_cast<unsigned char*>(d_ws) + rows_bytes;
+    const int rc = order_points(d_pts, n_pts, ob, ow, st);
+    if (rc != FE_OK) return rc;
+    d_pts = reinterpret_cast<const double*>(ob + ow.pts);
+    perm = reinterpret_cast<const int*>(ob + ow.perm);
+    used += ow.bytes;
+  }
   const int smem = FE_NSTAGE * FE_STAGE_BYTES;
   double* rows = static_cast<double*>(d_ws);
   auto next_rows = [&](int k) {
@@ -841,7 +907,7 @@ int eval_launch(const char* who, const void* d_table, const double* d_pts, int n
     FE_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     k1<<<dim3(g.nblk_x, g.split[1]), kEvalThreads, smem, st>>>(a);
   } else {
-    if (ws_bytes - rows_bytes < 4)
+    if (ws_bytes - used < 4)
       return fail(FE_ERR_SIZE, "%s: workspace has no room for the routing mask (size it with "
                   "fe_eval_ws_bytes_mixed)", who);
     FeMixedArgs a{};
@@ -851,8 +917,8 @@ int eval_launch(const char* who, const void* d_table, const double* d_pts, int n
     a.ld = g.ld;
     a.tau = float(tau);
     a.n64 = d_n64;
-    a.mask = reinterpret_cast<unsigned*>(static_cast<unsigned char*>(d_ws) + rows_bytes);
-    a.mask_words = static_cast<long long>((ws_bytes - rows_bytes) / 4);
+    a.mask = reinterpret_cast<unsigned*>(static_cast<unsigned char*>(d_ws) + used);
+    a.mask_words = static_cast<long long>((ws_bytes - used) / 4);
     a.lmin = lmin;
     a.lmax = lmax;
     auto f0 = fe_eval_f32_kernel<kMinB32Lo, 0, FE_MXSPLIT>;
@@ -873,7 +939,8 @@ int eval_launch(const char* who, const void* d_table, const double* d_pts, int n
   }
   FE_CUDA(cudaGetLastError());
   fe_reduce_kernel<<<(n_pts + 255) / 256, 256, 0, st>>>(tb, d_pts, n_pts, static_cast<double*>(d_ws),
-                                                        int(g.ws_rows()), g.ld, d_out, out_mode);
+                                                        int(g.ws_rows()), g.ld, d_out, out_mode,
+                                                        perm);
   FE_CUDA(cudaGetLastError());
   return FE_OK;
 }

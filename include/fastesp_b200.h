@@ -129,13 +129,25 @@ int fe_table_make_f32(void* d_table, cudaStream_t stream);
 int fe_table_info_get(const void* d_table, fe_table_info* info, cudaStream_t stream);
 
 /* Workspace bytes of an FP64 evaluation of n_pts points: the per-split
- * partial sums of the pair-split reduction. */
+ * partial sums of the pair-split reduction (the minimum; see
+ * fe_point_order_bytes). */
 size_t fe_eval_ws_bytes(int n_pts);
+
+/* Further workspace bytes with which the evaluators (fe_esp_fp64,
+ * fe_electron_fp64, fe_electron_classes at precision 0) take the points in a
+ * spatially coherent order -- a stable counting sort by the Morton code of a
+ * 32^3 grid of cells over the points' bounding box -- and write every result
+ * to its caller's row.  Faster for point sets in any order; the FP64 results
+ * are the same bit for bit either way (each point's sum runs over the pairs in
+ * table order whatever its neighbours).  fe_eval_ws_bytes_mixed includes them:
+ * the mixed path always evaluates in this order. */
+size_t fe_point_order_bytes(int n_pts);
 
 /* Workspace bytes of a mixed-precision evaluation of n_pts points of a table
  * holding at most cap[L] pairs of class L (fe_sizes.cap of its plan, or the
- * counts of an imported table): partial sums plus the FP64 routing mask (one
- * bit per pair and warp of points). */
+ * counts of an imported table): partial sums, the spatial point order
+ * (fe_point_order_bytes) and the FP64 routing mask (one bit per pair and warp
+ * of points). */
 size_t fe_eval_ws_bytes_mixed(int n_pts, const int* cap);
 
 /* V(C) = sum_A Z_A/|C-R_A| - sum_pairs K sum_k G_k R^alpha F_m(p R^2), all FP64,
