@@ -363,7 +363,9 @@ def run_ours(args):
     prof = ROOT / "profiles" / f"eval_{'mixed' if prec == 'mixed' else 'f64'}_frag54_30000.json"
     if prof.exists():
         traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
-    launches = 6 if prec == "mixed" else 3     # evaluator kernel instances + the reduction
+    # per step: the point order (bbox, count, scan, place, rank), the evaluator
+    # kernel instances and the reduction
+    launches = 5 + (6 if prec == "mixed" else 3)
     line = {
         "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,

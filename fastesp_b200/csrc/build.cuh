@@ -1250,40 +1250,41 @@ __global__ void __launch_bounds__(FE_SCAN_BLOCK) fe_scan_sums_kernel(
   }
 }
 
-// In-place exclusive scan of ``bsum`` (nb entries) by one block: every thread
-// sums its contiguous chunk, a shuffle scan over each warp and a scan of the
-// warp totals give the chunk offsets, then every thread writes its chunk.
+// In-place exclusive scan of ``bsum`` (nb entries) by one block, in tiles of
+// FE_SCAN_BLOCK consecutive entries (coalesced): a shuffle scan over each warp
+// and a scan of the warp totals give each entry's offset within the tile, and a
+// running carry the tiles before it.
 __global__ void __launch_bounds__(FE_SCAN_BLOCK) fe_scan_top_kernel(int* bsum, int nb) {
   __shared__ int wsum[FE_SCAN_BLOCK / 32];
+  __shared__ int tile_total;
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-  const int chunk = (nb + FE_SCAN_BLOCK - 1) / FE_SCAN_BLOCK;
-  const int c0 = min(t * chunk, nb), c1 = min(c0 + chunk, nb);
-  int tot = 0;
-  for (int i = c0; i < c1; ++i) tot += bsum[i];
-  int inc = tot;                                   // inclusive scan within the warp
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int v = __shfl_up_sync(0xffffffffu, inc, o);
-    if (lane >= o) inc += v;
-  }
-  if (lane == 31) wsum[w] = inc;
-  __syncthreads();
-  if (w == 0) {
-    int v = lane < FE_SCAN_BLOCK / 32 ? wsum[lane] : 0;
-    int x = v;
+  int carry = 0;
+  for (int base = 0; base < nb; base += FE_SCAN_BLOCK) {
+    const int i = base + t;
+    const int v = i < nb ? bsum[i] : 0;
+    int inc = v;                                   // inclusive scan within the warp
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const int u = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += u;
+      const int u = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += u;
     }
-    if (lane < FE_SCAN_BLOCK / 32) wsum[lane] = x - v;     // exclusive warp offsets
-  }
-  __syncthreads();
-  int run = wsum[w] + inc - tot;                   // exclusive offset of this chunk
-  for (int i = c0; i < c1; ++i) {
-    const int v = bsum[i];
-    bsum[i] = run;
-    run += v;
+    if (lane == 31) wsum[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+      const int x0 = lane < FE_SCAN_BLOCK / 32 ? wsum[lane] : 0;
+      int x = x0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += u;
+      }
+      if (lane < FE_SCAN_BLOCK / 32) wsum[lane] = x - x0;   // exclusive warp offsets
+      if (lane == 31) tile_total = x;
+    }
+    __syncthreads();
+    if (i < nb) bsum[i] = carry + wsum[w] + inc - v;
+    carry += tile_total;
+    __syncthreads();                               // wsum and tile_total are reused
   }
 }
 
