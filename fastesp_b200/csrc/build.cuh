@@ -1312,10 +1312,10 @@ __global__ void __launch_bounds__(FE_SCAN_BLOCK) fe_scan_apply_kernel(
 // far-pair test) and branch per warp (the Boys regimes), so a warp whose points
 // lie close together does less work than one spread over the molecule.  With
 // room in the workspace, the points are evaluated in the order of the Morton
-// code of a 32^3 grid of cells over their bounding box, in the caller's order
+// code of a 16^3 grid of cells over their bounding box, in the caller's order
 // within a cell (a stable counting sort: the order, and so every result, is
 // the same from run to run), and every result goes back to its caller's row.
-#define FE_ORDER_BITS 5
+#define FE_ORDER_BITS 4
 #define FE_ORDER_CELLS (1 << (3 * FE_ORDER_BITS))
 
 // idx: the points grouped by cell, in any order within a cell (``cursor``

@@ -136,7 +136,7 @@ size_t fe_eval_ws_bytes(int n_pts);
 /* Further workspace bytes with which the evaluators (fe_esp_fp64,
  * fe_electron_fp64, fe_electron_classes at precision 0) take the points in a
  * spatially coherent order -- a stable counting sort by the Morton code of a
- * 32^3 grid of cells over the points' bounding box -- and write every result
+ * 16^3 grid of cells over the points' bounding box -- and write every result
  * to its caller's row.  Faster for point sets in any order; the FP64 results
  * are the same bit for bit either way (each point's sum runs over the pairs in
  * table order whatever its neighbours).  fe_eval_ws_bytes_mixed includes them:
