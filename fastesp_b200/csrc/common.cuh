@@ -79,8 +79,9 @@ FE_DEV void fe_poison_row(double* row, int p0, int stride, int npts) {
   }
 }
 
-// 1-D TMA bulk copy global -> shared, completing on ``bar`` (no multicast).
-// dst/src 16-byte aligned, bytes a multiple of 16.
+// 1-D TMA bulk copy global -> shared, completing on ``bar``; the destination is
+// this block's own shared memory.  dst/src 16-byte aligned, bytes a multiple
+// of 16.
 FE_DEV void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
