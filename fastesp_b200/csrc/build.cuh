@@ -49,6 +49,8 @@ struct FeBuildArgs {
   int n_func;
   const double* dens;            // (n_func, n_func) Cartesian density
   const double* pts;             // (npts, 3)
+  const float4* ptsf;            // the same points rounded to float (x, y, z, 0)
+  const double* pbox;            // their bounding box: lo xyz, hi xyz
   int npts;
   const double* box;             // per 32-point block: lo xyz, hi xyz (6 doubles)
   const double* sbox;            // per 32-block superblock: the same
@@ -286,10 +288,11 @@ FE_DEV int fe_morton_cell(const double* __restrict__ q, const double* __restrict
   return code;
 }
 
-// cell[q] and the per-cell counts (2^(3 BITS) cells, counts zeroed by the caller).
+// cell[q] and the per-cell counts (2^(3 BITS) cells, counts zeroed by the caller);
+// bbp[6 FE_BBOX_BLOCKS ..] receives the combined bounding box.
 template <int BITS>
 __global__ void fe_points_count_kernel(const double* __restrict__ pts, int npts,
-                                       const double* __restrict__ bbp, int* __restrict__ cell,
+                                       double* __restrict__ bbp, int* __restrict__ cell,
                                        int* __restrict__ count) {
   __shared__ double bb[6];
   if (threadIdx.x < 6) {
@@ -297,6 +300,7 @@ __global__ void fe_points_count_kernel(const double* __restrict__ pts, int npts,
     for (int i = 0; i < FE_BBOX_BLOCKS; ++i)
       v = threadIdx.x < 3 ? fmin(v, bbp[6 * i + threadIdx.x]) : fmax(v, bbp[6 * i + threadIdx.x]);
     bb[threadIdx.x] = v;
+    if (blockIdx.x == 0) bbp[6 * FE_BBOX_BLOCKS + threadIdx.x] = v;   // the whole box
   }
   __syncthreads();
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -309,7 +313,7 @@ __global__ void fe_points_count_kernel(const double* __restrict__ pts, int npts,
 // ``cursor`` starts as the exclusive scan of the cell counts.
 __global__ void fe_points_place_kernel(const double* __restrict__ pts, int npts,
                                        const int* __restrict__ cell, int* __restrict__ cursor,
-                                       double* __restrict__ out) {
+                                       double* __restrict__ out, float4* __restrict__ outf) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= npts) return;
   const int at = atomicAdd(cursor + cell[q], 1);
@@ -319,6 +323,7 @@ __global__ void fe_points_place_kernel(const double* __restrict__ pts, int npts,
   }
 #pragma unroll
   for (int k = 0; k < 3; ++k) out[3 * at + k] = pts[3 * q + k];
+  outf[at] = make_float4(float(pts[3 * q]), float(pts[3 * q + 1]), float(pts[3 * q + 2]), 0.0f);
 }
 
 // E[i][j][t] of (u + xa)^i (u + xb)^j exp(-p u^2), i <= LA, j <= LB, t <= LA+LB.
@@ -408,6 +413,34 @@ struct FeScreen {
   }
 };
 
+// FP32 pre-test of the point screens.  With every coordinate of the points and
+// of P rounded to float (error at most eps M, eps = 2^-24, M the largest
+// coordinate magnitude of the points' box and of P), the FP32 distance of a
+// point within rcut of P -- three roundings in the difference, three in the
+// sum of squares -- is below (rcut + 4 eps M)(1 + 4 eps).  A point whose FP32
+// squared distance exceeds that bound, rounded up to float, lies beyond rcut
+// and is skipped; the others get the exact FP64 test, so the screen's
+// minimum over the points within rcut, and its decision, are unchanged.
+struct FeScreenF32 {
+  float px, py, pz, r2f;
+  FE_DEV FeScreenF32(const FeBuildArgs& a, const double (&P)[3], double rcut2) {
+    double M = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      M = fmax(M, fmax(fabs(P[k]), fmax(fabs(a.pbox[k]), fabs(a.pbox[3 + k]))));
+    const double eps = 5.9604644775390625e-08;
+    const double rf = (sqrt(rcut2) + 4.0 * eps * M) * (1.0 + 4.0 * eps);
+    px = float(P[0]);
+    py = float(P[1]);
+    pz = float(P[2]);
+    r2f = __double2float_ru(rf * rf);
+  }
+  FE_DEV bool maybe_within(float4 q) const {
+    const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+    return fmaf(dx, dx, fmaf(dy, dy, dz * dz)) <= r2f;
+  }
+};
+
 // One thread's screen with a budget of FE_SCREEN_BUDGET box/point tests:
 // 0 dropped, 1 kept, 2 undecided (the warp-parallel screen finishes it).
 // (Not inlining it -- one copy for the 25 (la, lb) instances -- was measured:
@@ -418,6 +451,7 @@ FE_DEV int fe_screen_thread(const FeBuildArgs& a, double px, double py, double p
   if (a.npts == 0 || a.tol <= 0.0) return 1;        // no points, or tol 0: every pair is kept
   const FeScreen sc(a, KB, reff);
   if (sc.none) return 0;
+  const FeScreenF32 sf(a, P, sc.rcut2);
   double d2min = 1e300;
   int steps = 0;
   for (int sb = 0; sb < a.nsbox; ++sb) {
@@ -434,6 +468,7 @@ FE_DEV int fe_screen_thread(const FeBuildArgs& a, double px, double py, double p
       const int q1 = min(32 * b + 32, a.npts);
       steps += q1 - 32 * b;
       for (int q = 32 * b; q < q1; ++q) {
+        if (!sf.maybe_within(a.ptsf[q])) continue;
         const double d2 = FeScreen::dist2(a.pts + 3 * q, P);
         if (d2 <= sc.rcut2) d2min = fmin(d2min, d2);
       }
@@ -640,6 +675,7 @@ FE_DEV long long fe_build_pair(const FeBuildArgs& a, int w) {
 // comes back in every lane.
 FE_DEV bool fe_screen_warp(const FeBuildArgs& a, const double (&P)[3], const FeScreen& sc,
                            int lane) {
+  const FeScreenF32 sf(a, P, sc.rcut2);
   double d2min = 1e300;
   bool sure = sc.none;                        // (cannot happen: its thread searched)
   for (int sb0 = 0; sb0 < a.nsbox && !sure; sb0 += 32) {
@@ -669,6 +705,7 @@ FE_DEV bool fe_screen_warp(const FeBuildArgs& a, const double (&P)[3], const FeS
             const int q1 = min(32 * b + 32, a.npts);
 #pragma unroll 8
             for (int q = 32 * b; q < q1; ++q) {
+              if (!sf.maybe_within(a.ptsf[q])) continue;
               const double d2 = FeScreen::dist2(a.pts + 3 * q, P);
               if (d2 <= sc.rcut2) dl = fmin(dl, d2);
             }

@@ -573,7 +573,7 @@ namespace {
 // boxes, superboxes, the spatially sorted screen points, their cells, the
 // cell counters (FE_SORT_CELLS + 1) and the points' bounding box.
 struct ScreenWs {
-  size_t box, sbox, sorted, cell, count, bb, bytes;
+  size_t box, sbox, sorted, sortedf, cell, count, bb, bytes;
 };
 ScreenWs screen_ws(size_t base, int n_pts) {
   const size_t nbox = (size_t(n_pts) + 31) / 32, nsbox = (nbox + 31) / 32;
@@ -583,9 +583,10 @@ ScreenWs screen_ws(size_t base, int n_pts) {
   w.box = put(nbox * 6 * sizeof(double));
   w.sbox = put(nsbox * 6 * sizeof(double));
   w.sorted = put(size_t(n_pts) * 3 * sizeof(double));
+  w.sortedf = put(size_t(n_pts) * sizeof(float4));
   w.cell = put(size_t(n_pts) * sizeof(int));
   w.count = put((FE_SORT_CELLS + 1) * sizeof(int));
-  w.bb = put(6 * FE_BBOX_BLOCKS * sizeof(double));
+  w.bb = put(6 * (FE_BBOX_BLOCKS + 1) * sizeof(double));     // partials, then the whole box
   w.bytes = o;
   return w;
 }
@@ -654,9 +655,13 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
     fe_points_bbox_kernel<<<FE_BBOX_BLOCKS, 256, 0, st>>>(d_pts, n_pts, bb);
     fe_points_count_kernel<4><<<(n_pts + 255) / 256, 256, 0, st>>>(d_pts, n_pts, bb, cell, count);
     fe_scan_top_kernel<<<1, FE_SCAN_BLOCK, 0, st>>>(count, FE_SORT_CELLS);
-    fe_points_place_kernel<<<(n_pts + 255) / 256, 256, 0, st>>>(d_pts, n_pts, cell, count, sorted);
+    float4* sortedf = reinterpret_cast<float4*>(wb + pw.sortedf);
+    fe_points_place_kernel<<<(n_pts + 255) / 256, 256, 0, st>>>(d_pts, n_pts, cell, count, sorted,
+                                                                sortedf);
     FE_CUDA(cudaGetLastError());
     a.pts = sorted;
+    a.ptsf = sortedf;
+    a.pbox = bb + 6 * FE_BBOX_BLOCKS;
     // one warp per box and per superbox
     fe_point_boxes_kernel<<<(a.nbox + 3) / 4, 128, 0, st>>>(sorted, n_pts, box, a.nbox);
     fe_super_boxes_kernel<<<(a.nsbox + 3) / 4, 128, 0, st>>>(box, a.nbox, sbox, a.nsbox);
@@ -803,7 +808,7 @@ OrderWs order_ws(int n) {
   w.idx = put(size_t(n) * sizeof(int));
   w.start = put((FE_ORDER_CELLS + 1) * sizeof(int));
   w.end = put((FE_ORDER_CELLS + 1) * sizeof(int));
-  w.bb = put(6 * FE_BBOX_BLOCKS * sizeof(double));
+  w.bb = put(6 * (FE_BBOX_BLOCKS + 1) * sizeof(double));    // partials, then the whole box
   w.bytes = o;
   return w;
 }

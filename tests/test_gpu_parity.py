@@ -143,6 +143,8 @@ def test_evaluate_reference_format_table(tmp_path, tz6_system):
     np.testing.assert_allclose(gt.esp(), ot.esp(), rtol=0, atol=1e-12)
     pts2 = g["points"][::7] + 0.37
     np.testing.assert_allclose(gt.esp(pts2), ot.esp(pts2), rtol=0, atol=1e-12)
+    # the imported table's FP32 records are derived on the device (fe_table_make_f32)
+    np.testing.assert_allclose(gt.esp(precision="mixed"), ot.esp(), rtol=0, atol=1e-6)
 
 
 def test_export_reference_format_table(tmp_path, small_system):
@@ -360,3 +362,36 @@ def test_every_workspace_row_is_written(frag54, npts, prec):
     assert np.isfinite(got).all()
     ref = tab.esp(pts, precision=prec)
     np.testing.assert_array_equal(got, ref)
+
+
+def test_point_order_keeps_rows_and_fp64_bits(frag54, golden):
+    """The evaluators' spatial point order (fe_point_order_bytes): the FP64 values
+    are the same bit for bit with and without the order's workspace, every value
+    lands in its caller's row (a permuted point set gives the permuted values,
+    bit for bit in FP64), and the mixed path stays within its bound."""
+    import torch
+    wfn, basis, P = frag54
+    g = golden("frag54_300")
+    tab = build_table(wfn, basis, P, g["points"], tol=1e-12)
+    n = len(g["points"])
+    L = _lib.lib()
+    pd = torch.as_tensor(g["points"], device="cuda")
+    perm = np.random.default_rng(5).permutation(n)
+    pp = torch.as_tensor(g["points"][perm], device="cuda")
+    bare = int(L.fe_eval_ws_bytes(n))
+    full = bare + int(L.fe_point_order_bytes(n))
+    assert full > bare
+
+    def fp64(points, nbytes):
+        ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+        out = torch.empty(n, dtype=torch.float64, device="cuda")
+        _lib.check(L.fe_esp_fp64(_lib.ptr(tab._buf), _lib.ptr(points), n, _lib.ptr(out),
+                                 _lib.ptr(ws), nbytes, _lib.stream_ptr()))
+        return out.cpu().numpy()
+    caller_order = fp64(pd, bare)
+    spatial = fp64(pd, full)
+    np.testing.assert_array_equal(spatial, caller_order)
+    np.testing.assert_array_equal(fp64(pp, full), spatial[perm])
+    assert np.abs(spatial - g["esp_t12"]).max() <= 1e-10
+    vm = tab.esp(pp, precision="mixed").cpu().numpy()
+    assert np.abs(vm - spatial[perm]).max() <= MIXED_TOL
