@@ -102,7 +102,9 @@ unsigned long long current_ctx_id() {
 // caller's stream waits for all of them.  Created on first use; a device reset
 // (a new context ID) makes them be created again.  The mutex is held from the
 // fork to the join, so concurrent builds on one device take turns on them.
+#ifndef FE_SIDE_STREAMS
 #define FE_SIDE_STREAMS 8
+#endif
 #define FE_SIDE_MAX_DEVICES 128
 struct SideStreams {
   cudaStream_t s[FE_SIDE_STREAMS] = {};
