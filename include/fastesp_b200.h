@@ -105,7 +105,12 @@ size_t fe_build_ws_bytes(const fe_plan* plan, int n_pts);
  * Cartesian density, ``d_pts`` the (n_pts, 3) points (Bohr) used for the
  * screen, ``rule`` FE_RULE_NUMPY or FE_RULE_NATIVE.  Replaces the hot loop and
  * output of build_pairs (build_pairs.cpp:194-421) and build_table
- * (fastesp/table.py:176-259). */
+ * (fastesp/table.py:176-259).  Stream-ordered on ``stream``: the per-(la, lb)
+ * group kernels and the per-class record kernels run on the library's own
+ * side streams of the device, forked from ``stream`` by an event and joined
+ * back into it, so they start after the work already on ``stream`` and every
+ * later launch on ``stream`` waits for them (capturable into a CUDA graph).
+ * Calls from several host threads take turns on the side streams. */
 int fe_table_build(const fe_plan* plan, const void* d_plan, const double* d_dens,
                    const double* d_pts, int n_pts, double tol, int rule,
                    void* d_table, void* d_ws, size_t ws_bytes, cudaStream_t stream);
