@@ -109,8 +109,8 @@ size_t fe_build_ws_bytes(const fe_plan* plan, int n_pts);
  * group kernels and the per-class record kernels run on the library's own
  * side streams of the device, forked from ``stream`` by an event and joined
  * back into it, so they start after the work already on ``stream`` and every
- * later launch on ``stream`` waits for them (capturable into a CUDA graph).
- * Calls from several host threads take turns on the side streams. */
+ * later launch on ``stream`` waits for them.  Calls from several host threads
+ * take turns on the side streams. */
 int fe_table_build(const fe_plan* plan, const void* d_plan, const double* d_dens,
                    const double* d_pts, int n_pts, double tol, int rule,
                    void* d_table, void* d_ws, size_t ws_bytes, cudaStream_t stream);
