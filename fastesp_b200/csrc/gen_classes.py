@@ -662,19 +662,6 @@ def main() -> int:
         out.append(f"__constant__ short fe_gpos_L{L}[{H.n_terms(L)}] = {{"
                    + ", ".join(str(pos[k]) for k in range(H.n_terms(L))) + "};")
     out.append("")
-    offs, cs, nms = [], [], []
-    for L in range(LMAX + 1):
-        offs.append(len(cs))
-        for n, m, c in route_constants(L):
-            cs.append(c)
-            nms.append(n | (m << 4))
-    out.append("// mixed-path routing bound: record position j of class L has constant")
-    out.append("// fe_route_c[fe_route_off[L] + j] and n | m << 4 in fe_route_nm (n = 2m - |a|)")
-    out.append("__constant__ int fe_route_off[FE_NCLASS] = {" + ", ".join(map(str, offs)) + "};")
-    out.append(f"__constant__ double fe_route_c[{len(cs)}] = {{" + ", ".join(repr(c) for c in cs) + "};")
-    out.append(f"__constant__ unsigned char fe_route_nm[{len(nms)}] = {{"
-               + ", ".join(map(str, nms)) + "};")
-    out.append("")
     out.append("static constexpr int fe_class_polyops[FE_NCLASS] = {"
                + ", ".join(map(str, nops)) + "};")
     out.append("")
