@@ -1371,6 +1371,9 @@ __global__ void fe_order_place_kernel(const int* __restrict__ cell, int npts,
 
 // Point q's final position: its cell's first position plus the number of the
 // cell's points with a smaller caller index.  sorted[pos] = pts[q], perm[pos] = q.
+// Each point scans its cell's segment, n^2 / 4096 comparisons for n evenly
+// spread points: 80 M at the 568,950-point grid (tens of microseconds), small
+// against the evaluation, which grows as n times the pair count.
 __global__ void fe_order_rank_kernel(const double* __restrict__ pts, int npts,
                                      const int* __restrict__ cell, const int* __restrict__ start,
                                      const int* __restrict__ end, const int* __restrict__ idx,
