@@ -665,8 +665,8 @@ FE_DEV long long fe_build_pair(const FeBuildArgs& a, int w) {
 // The screen of one pair that its thread left undecided (fe_screen_thread ran
 // past its budget), by the 32 lanes of a warp that all pass the same slot:
 // superboxes across the lanes; then, one candidate superbox at a time, its
-// boxes across the lanes, each lane testing every point of its box if the
-// box's bounds leave it a candidate.  The decision is the serial search's:
+// boxes across the lanes, and the points of the boxes whose bounds leave them
+// candidates, one box at a time across the lanes.  The decision is the serial search's:
 // it depends only on whether some candidate box lies wholly within the keep
 // radius (sure_box) and on the minimum squared distance over the points
 // within rcut, which the box bounds only prune -- a box whose lower bound
@@ -694,27 +694,29 @@ FE_DEV bool fe_screen_warp(const FeBuildArgs& a, const double (&P)[3], const FeS
         break;
       }
       const int b = 32 * sbi + lane;
-      bool bsure = false;
-      double dl = 1e300;
+      bool bsure = false, bc = false;
       if (b < a.nbox) {
         const double lb = fe_box_lb2(a.box + 6 * b, P) * (1.0 - 1e-12);
         if (lb <= sc.rcut2 && lb <= d2min) {
-          if (sc.sure_box(fe_box_ub2(a.box + 6 * b, P))) {
-            bsure = true;
-          } else {
-            const int q1 = min(32 * b + 32, a.npts);
-#pragma unroll 8
-            for (int q = 32 * b; q < q1; ++q) {
-              if (!sf.maybe_within(a.ptsf[q])) continue;
-              const double d2 = FeScreen::dist2(a.pts + 3 * q, P);
-              if (d2 <= sc.rcut2) dl = fmin(dl, d2);
-            }
-          }
+          if (sc.sure_box(fe_box_ub2(a.box + 6 * b, P))) bsure = true;
+          else bc = true;
         }
       }
       if (__any_sync(0xffffffffu, bsure)) {
         sure = true;
         break;
+      }
+      // the candidate boxes' points, one box at a time across the lanes
+      // (coalesced), the minimum reduced once for the superbox
+      double dl = 1e300;
+      unsigned bm = __ballot_sync(0xffffffffu, bc);
+      while (bm) {
+        const int q = 32 * (32 * sbi + __ffs(bm) - 1) + lane;
+        bm &= bm - 1;
+        if (q < a.npts && sf.maybe_within(a.ptsf[q])) {
+          const double d2 = FeScreen::dist2(a.pts + 3 * q, P);
+          if (d2 <= sc.rcut2) dl = fmin(dl, d2);
+        }
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) dl = fmin(dl, __shfl_xor_sync(0xffffffffu, dl, o));
