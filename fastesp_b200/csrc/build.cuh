@@ -950,17 +950,23 @@ __host__ __device__ constexpr bool fe_warp_pair_group(int la, int lb) {
   return (la + 1) * (la + 2) / 2 * ((lb + 1) * (lb + 2) / 2) >= FE_WARP_PAIR_MIN;
 }
 
+// Threads per block of fe_build_warp_kernel (one pair per warp).
+#define FE_WARP_BLOCK 128
+
 template <int LA, int LB>
-__global__ void __launch_bounds__(128) fe_build_warp_kernel(const FeBuildArgs a, int work0,
-                                                            int nwork) {
+__global__ void __launch_bounds__(FE_WARP_BLOCK) fe_build_warp_kernel(const FeBuildArgs a,
+                                                                     int work0, int nwork) {
   constexpr int SH = fe_warp_pair_smem<LA, LB>();
-  __shared__ double sh[4 * SH];
+  constexpr int NW = FE_WARP_BLOCK / 32;
+  __shared__ double sh[NW * SH];
   const int wid = int(threadIdx.x >> 5);
-  const int w = int(blockIdx.x) * 4 + wid;
+  const int w = int(blockIdx.x) * NW + wid;
   if (w < nwork) fe_build_pair_warp<LA, LB>(a, work0 + w, int(threadIdx.x & 31), sh + wid * SH);
 }
 
+#ifndef FE_BUILD_THREADS
 #define FE_BUILD_THREADS 128
+#endif
 
 // One launch per (la, lb) group of work items (all primitive pairs of the
 // shell pairs with these angular momenta): each group's code gets its own
@@ -1004,7 +1010,7 @@ __global__ void __launch_bounds__(128) fe_screen_pending_kernel(const FeBuildArg
 using FeBuildKernel = void (*)(const FeBuildArgs, int, int);
 
 // The kernel of group la * 5 + lb: fe_build_warp_kernel (one warp per pair,
-// FE_BUILD_THREADS / 32 pairs per block) for the heavy groups,
+// FE_WARP_BLOCK / 32 pairs per block) for the heavy groups,
 // fe_build_kernel (one thread per pair) for the rest.
 template <int LA, int LB>
 constexpr FeBuildKernel fe_group_kernel() {
@@ -1022,9 +1028,12 @@ inline FeBuildKernel fe_build_kernel_for(int code) {
 #undef FE_K
   return code >= 0 && code < 25 ? k[code] : nullptr;
 }
-// Pairs per block of group la * 5 + lb's kernel.
+// Threads and pairs per block of group la * 5 + lb's kernel.
+inline int fe_build_block_threads(int code) {
+  return fe_warp_pair_group(code / 5, code % 5) ? FE_WARP_BLOCK : FE_BUILD_THREADS;
+}
 inline int fe_build_pairs_per_block(int code) {
-  return fe_warp_pair_group(code / 5, code % 5) ? FE_BUILD_THREADS / 32 : FE_BUILD_THREADS;
+  return fe_warp_pair_group(code / 5, code % 5) ? FE_WARP_BLOCK / 32 : FE_BUILD_THREADS;
 }
 
 // log2(x) for finite x > 0 and 2^y to about 1e-6 relative (float MUFU on the

@@ -676,12 +676,13 @@ int fe_table_build(const fe_plan* p, const void* d_plan, const double* d_dens,
     // while the warp-per-pair groups (which leave none) run beside them
     std::vector<int> tg, wg;
     for (int g = 0; g < int(p->grp_code.size()); ++g)
-      (fe_build_pairs_per_block(p->grp_code[g]) == FE_BUILD_THREADS ? tg : wg).push_back(g);
+      (fe_warp_pair_group(p->grp_code[g] / 5, p->grp_code[g] % 5) ? wg : tg).push_back(g);
     auto group = [&](int g, cudaStream_t sg) {
       const FeBuildKernel k = fe_build_kernel_for(p->grp_code[g]);
       if (!k) return fail(FE_ERR_ARG, "table build: bad group code %d", p->grp_code[g]);
       const int nw = p->grp_nwork[g], per = fe_build_pairs_per_block(p->grp_code[g]);
-      k<<<unsigned((nw + per - 1) / per), FE_BUILD_THREADS, 0, sg>>>(a, p->grp_work0[g], nw);
+      k<<<unsigned((nw + per - 1) / per), fe_build_block_threads(p->grp_code[g]), 0, sg>>>(
+          a, p->grp_work0[g], nw);
       FE_CUDA(cudaGetLastError());
       return FE_OK;
     };
